@@ -1,0 +1,141 @@
+// Library-wide C entry points (version, errors, synchronisation, zdtutils.jl helpers) and
+// the internal host utilities declared in fdr_internal.cuh.
+#include <stdarg.h>
+#include <string.h>
+
+#include <atomic>
+#include <mutex>
+
+#include "fdr_internal.cuh"
+
+namespace fdr {
+
+static thread_local std::string g_last_error;
+static std::atomic<long long> g_launches{0};
+
+void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+void set_error(int status, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = std::string(fdr_status_string(status)) + ": " + buf;
+}
+
+int cuda_status(cudaError_t e, const char* what) {
+  int st = (e == cudaErrorMemoryAllocation) ? FDR_ERR_OUT_OF_MEMORY
+           : (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) ? FDR_ERR_NO_DEVICE
+                                                                          : FDR_ERR_CUDA;
+  // Clear a non-sticky error so later calls on this thread start clean.
+  (void)cudaGetLastError();
+  set_error(st, "%s failed: %s (%s)", what, cudaGetErrorName(e), cudaGetErrorString(e));
+  return st;
+}
+
+int64_t nextprod(const int64_t* factors, int nfactors, int64_t n) {
+  static const int64_t deflt[3] = {2, 3, 5};
+  if (factors == nullptr || nfactors <= 0) { factors = deflt; nfactors = 3; }
+  for (int i = 0; i < nfactors; ++i)
+    if (factors[i] < 2) return -1;
+  if (n <= 1) return 1;
+  // Smallest product of powers of the factors that is >= n, by depth-first search over the
+  // exponents (the search space is tiny for the sizes used here).
+  int64_t best = INT64_MAX;
+  struct Rec {
+    const int64_t* f;
+    int nf;
+    int64_t n;
+    int64_t* best;
+    void go(int i, int64_t cur) {
+      if (cur >= n) { if (cur < *best) *best = cur; return; }
+      if (i == nf) return;
+      int64_t v = cur;
+      while (true) {
+        go(i + 1, v);
+        if (v >= n || v > INT64_MAX / f[i]) break;
+        v *= f[i];
+      }
+    }
+  } r{factors, nfactors, n, &best};
+  r.go(0, 1);
+  return best == INT64_MAX ? -1 : best;
+}
+
+int scratch_alloc(void** p, size_t bytes, cudaStream_t s) {
+  *p = nullptr;
+  if (bytes == 0) return FDR_OK;
+  FDR_CUDA(cudaMallocAsync(p, bytes, s));
+  return FDR_OK;
+}
+
+void scratch_free(void* p, cudaStream_t s) {
+  if (p) cudaFreeAsync(p, s);
+}
+
+int sm_count() {
+  static int cached[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+  if (dev < 64 && cached[dev]) return cached[dev];
+  int n = 0;
+  if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
+    n = 148;
+  if (dev < 64) cached[dev] = n;
+  return n;
+}
+
+}  // namespace fdr
+
+extern "C" {
+
+const char* fdr_version(void) { return "fdr_b200 0.1.0 (sm_100a)"; }
+
+const char* fdr_last_error_string(void) { return fdr::g_last_error.c_str(); }
+
+int64_t fdr_kernel_launches(void) { return fdr::g_launches.load(std::memory_order_relaxed); }
+
+const char* fdr_status_string(int status) {
+  switch (status) {
+    case FDR_OK: return "FDR_OK";
+    case FDR_ERR_INVALID_ARGUMENT: return "FDR_ERR_INVALID_ARGUMENT";
+    case FDR_ERR_UNSUPPORTED_SIZE: return "FDR_ERR_UNSUPPORTED_SIZE";
+    case FDR_ERR_UNSUPPORTED_WINDOW: return "FDR_ERR_UNSUPPORTED_WINDOW";
+    case FDR_ERR_OUT_OF_MEMORY: return "FDR_ERR_OUT_OF_MEMORY";
+    case FDR_ERR_CUDA: return "FDR_ERR_CUDA";
+    case FDR_ERR_CAPACITY: return "FDR_ERR_CAPACITY";
+    case FDR_ERR_NO_DEVICE: return "FDR_ERR_NO_DEVICE";
+    default: return "FDR_ERR_UNKNOWN";
+  }
+}
+
+int fdr_synchronize(fdr_stream_t stream) {
+  if (stream) {
+    FDR_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+  } else {
+    FDR_CUDA(cudaDeviceSynchronize());
+  }
+  return FDR_OK;
+}
+
+int64_t fdr_calc_nl(int64_t Nt, int64_t Nr, const int64_t* factors, int nfactors) {
+  if (Nt < 1 || Nr < 1) return -1;
+  return fdr::nextprod(factors, nfactors, Nt + Nr - 1);
+}
+
+int64_t fdr_grow_nr(int64_t Nt, int64_t Nr, const int64_t* factors, int nfactors) {
+  int64_t nl = fdr_calc_nl(Nt, Nr, factors, nfactors);
+  return nl < 0 ? -1 : nl - Nt + 1;
+}
+
+int64_t fdr_estimate_memory(int64_t Nf, int64_t Nt, int64_t Nr, int64_t Ni, int64_t No,
+                            const int64_t* factors, int nfactors) {
+  int64_t Nl = fdr_calc_nl(Nt, Nr, factors, nfactors);
+  if (Nl < 0 || Nf < 1) return -1;
+  Ni += 3;
+  const int64_t Nz = 3;
+  return 4 * ((Nf * Nt) * Ni + (Nf * Nl) * Nz + (Nf * Nr) * No);
+}
+
+}  // extern "C"

@@ -1,0 +1,112 @@
+// Internal helpers shared by the FDR CUDA translation units (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string>
+#include <vector>
+
+#include "../../include/fdr_b200.h"
+
+namespace fdr {
+
+// ------------------------------------------------------------------------------------
+// Error reporting: every C entry point returns an fdr_status; the message of the last
+// failure on the calling host thread is kept for fdr_last_error_string().
+// ------------------------------------------------------------------------------------
+void set_error(int status, const char* fmt, ...);
+int cuda_status(cudaError_t e, const char* what);
+
+#define FDR_CHECK_ARG(cond, ...)                                              \
+  do {                                                                        \
+    if (!(cond)) {                                                            \
+      fdr::set_error(FDR_ERR_INVALID_ARGUMENT, __VA_ARGS__);                  \
+      return FDR_ERR_INVALID_ARGUMENT;                                        \
+    }                                                                         \
+  } while (0)
+
+#define FDR_CUDA(call)                                                        \
+  do {                                                                        \
+    cudaError_t e__ = (call);                                                 \
+    if (e__ != cudaSuccess) return fdr::cuda_status(e__, #call);              \
+  } while (0)
+
+#define FDR_TRY(call)                                                         \
+  do {                                                                        \
+    int s__ = (call);                                                         \
+    if (s__ != FDR_OK) return s__;                                            \
+  } while (0)
+
+// Counts a kernel launch (fdr_kernel_launches) and checks the launch error; placed after
+// every <<<>>> launch of the library.
+void count_launch(int n = 1);
+#define FDR_LAUNCH_CHECK(what)                                                \
+  do {                                                                        \
+    fdr::count_launch();                                                      \
+    FDR_CUDA(cudaPeekAtLastError());                                          \
+  } while (0)
+
+// ------------------------------------------------------------------------------------
+// Complex helpers (float2 = complex64 with .x real, .y imaginary)
+// ------------------------------------------------------------------------------------
+__host__ __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__host__ __device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
+__host__ __device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+// multiply by +i (s=+1) or -i (s=-1)
+__host__ __device__ __forceinline__ float2 cmul_i(float2 a, int s) {
+  return s > 0 ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+// (a.x + i a.y) * (b.x + i b.y) with each product rounded separately and no FMA
+// contraction, as Julia's ComplexF32 `*` computes it.
+__device__ __forceinline__ float2 cmul_rn(float2 a, float2 b) {
+  return make_float2(__fsub_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)),
+                     __fadd_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x)));
+}
+
+// cispi(x) = exp(i*pi*x) for a float argument (CUDA's sincospif reduces x exactly).
+__device__ __forceinline__ float2 cispif(float x) {
+  float s, c;
+  sincospif(x, &s, &c);
+  return make_float2(c, s);
+}
+
+// exp(i*pi*h) where h = num / den half-turns is given exactly as an integer fraction
+// reduced in integer arithmetic: the residue (num mod 2*den) is exact, only the final
+// conversion of the residue to a float in [-1, 1) rounds.
+__device__ __forceinline__ float2 cispi_frac(long long num, long long den2 /* = 2*den */) {
+  long long r = num % den2;
+  if (r < 0) r += den2;
+  // h = 2*r/den2 in [0, 2); map to [-1, 1)
+  double h = 2.0 * (double)r / (double)den2;
+  if (h >= 1.0) h -= 2.0;
+  return cispif((float)h);
+}
+
+// exp(i*pi*h) for a double h reduced modulo 2 in double precision first.
+__device__ __forceinline__ float2 cispi_d(double h) {
+  double r = h - 2.0 * rint(0.5 * h);
+  return cispif((float)r);
+}
+
+// ------------------------------------------------------------------------------------
+// Small host utilities
+// ------------------------------------------------------------------------------------
+int64_t nextprod(const int64_t* factors, int nfactors, int64_t n);
+bool factorize(int64_t n, std::vector<int>& radices, int max_prime);
+inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
+inline bool is_pow2(int64_t n) { return n > 0 && (n & (n - 1)) == 0; }
+inline int ilog2(int64_t n) { int l = 0; while ((int64_t(1) << l) < n) ++l; return l; }
+
+// Temporary device memory from the stream-ordered pool.
+int scratch_alloc(void** p, size_t bytes, cudaStream_t s);
+void scratch_free(void* p, cudaStream_t s);
+
+// Current device's SM count (cached per device).
+int sm_count();
+
+}  // namespace fdr

@@ -1,0 +1,95 @@
+"""FDR utilities (src/fdrutils.jl) over the C ABI."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib
+from .arrays import as_device_f32, fortran_empty, ptr, stream_handle
+
+
+def _mats(fdr):
+    if isinstance(fdr, torch.Tensor):
+        return [fdr], True
+    return list(fdr), False
+
+
+def _ptr_array(mats):
+    return (C.c_void_p * len(mats))(*[m.data_ptr() for m in mats])
+
+
+def create_fdr(spectrogram, Nr_or_rates):
+    """create_fdr (fdrutils.jl:11-26): uninitialised (Nf, Nr) float32 device matrix."""
+    Nr = Nr_or_rates if isinstance(Nr_or_rates, int) else len(Nr_or_rates)
+    return fortran_empty(spectrogram.shape[0], Nr)
+
+
+def fdrstats(fdr, stream=None):
+    """fdrstats (fdrutils.jl:39-50) -> (m, s) as float32 values (the reference's types);
+    accumulated in float64 on the device."""
+    mats, _ = _mats(fdr)
+    Nf, Nrb = mats[0].shape
+    m, s = C.c_double(), C.c_double()
+    _lib.check(_lib.lib().fdr_stats(_ptr_array(mats), len(mats), Nf, Nrb, C.byref(m),
+                                    C.byref(s), stream_handle(stream)))
+    return np.float32(m.value), np.float32(s.value)
+
+
+def fdrnormalize(x, m, s):
+    """fdrnormalize(scalar, m, s) (fdrutils.jl:65-68)."""
+    return (x - m) / s
+
+
+def fdrnormalize_(fdr, m=None, s=None, stream=None):
+    """fdrnormalize! (fdrutils.jl:70-90), in place on one matrix or a list of them."""
+    mats, single = _mats(fdr)
+    if m is None or s is None:
+        m, s = fdrstats(fdr, stream)
+    Nf, Nrb = mats[0].shape
+    _lib.check(_lib.lib().fdr_normalize(_ptr_array(mats), len(mats), Nf, Nrb,
+                                        float(np.float32(m)), float(np.float32(s)),
+                                        stream_handle(stream)))
+    return fdr
+
+
+def fdrdenormalize(snr, m_or_fdr, s=None, stream=None):
+    """fdrdenormalize (fdrutils.jl:104-119)."""
+    if s is None:
+        m, s = fdrstats(m_or_fdr, stream)
+    else:
+        m = m_or_fdr
+    return snr * float(s) + float(m)
+
+
+def fdrsynchronize(_type=None):
+    """fdrsynchronize (fdrutils.jl:129-130; CuArray method ext:26-28)."""
+    _lib.check(_lib.lib().fdr_synchronize(C.c_void_p(None)))
+
+
+def findprotohits(fdr, threshold, snr=False, capacity=None, stream=None, return_threshold=False):
+    """findprotohits (fdrutils.jl:148-169) -> int64 numpy array (nhits, 2) of ZERO-based
+    (i, j) in column-major order (j offset by b*Nrb for the b-th matrix of a list)."""
+    mats, _ = _mats(fdr)
+    Nf, Nrb = mats[0].shape
+    for mm in mats:
+        if tuple(mm.shape) != (Nf, Nrb):
+            raise _lib.FDRError(_lib.FDR_ERR_INVALID_ARGUMENT, "matrices differ in size")
+    if capacity is None:
+        capacity = 1 << 20
+    while True:
+        hits = torch.empty((max(1, capacity), 2), dtype=torch.int64, device="cuda")
+        count = C.c_int64()
+        thr = C.c_double()
+        st = _lib.lib().fdr_findprotohits(_ptr_array(mats), len(mats), Nf, Nrb,
+                                          float(threshold), 1 if snr else 0, ptr(hits),
+                                          capacity, C.byref(count), C.byref(thr),
+                                          stream_handle(stream))
+        if st == _lib.FDR_ERR_CAPACITY:
+            capacity = int(count.value)
+            continue
+        _lib.check(st)
+        break
+    out = hits[: count.value].cpu().numpy()
+    return (out, thr.value) if return_threshold else out

@@ -1,0 +1,217 @@
+/*
+ * fdr_b200.h -- C ABI of the B200-native frequency-drift-rate (FDR) transform library
+ * (libfdrb200.so).
+ *
+ * This is the drop-in boundary for FrequencyDriftRateTransforms.jl's GPU path: the
+ * reference specialises three generics for CuArrays in
+ * ext/CUDAFrequencyDriftRateTransformsExt.jl (plan_ffts! :50-82, output! :94-103,
+ * fdrsynchronize :26-28) and runs every other stage as CUDA.jl broadcasts.  A Julia
+ * extension that ccalls this library replaces all of them; each entry point below names
+ * the reference function it stands in for.
+ *
+ * Conventions
+ *  - Every function returns an fdr_status (0 = FDR_OK).  On failure,
+ *    fdr_last_error_string() describes the last error of the calling host thread.
+ *    Nonzero statuses correspond to the reference's thrown errors (@assert, error(...)).
+ *  - Arrays are Julia column-major: an Nf x Nt spectrogram has channel (frequency) index
+ *    fastest; element (n, t) of a matrix with leading dimension ld is at p[n + t*ld].
+ *    Complex arrays are interleaved float pairs (ComplexF32).
+ *  - Array arguments are DEVICE pointers unless the parameter says "host".
+ *  - Work is ordered on the given CUDA stream (NULL = the legacy default stream) and is
+ *    asynchronous unless the function says it synchronises (those that return values
+ *    computed on the device to host variables).
+ *  - Element type is Float32 (the reference is generic over Real element types; this
+ *    library implements Float32 only).
+ *  - Indices returned to the caller are ZERO-based (the Julia shim adds 1).
+ */
+#ifndef FDR_B200_H
+#define FDR_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* cudaStream_t-compatible handle. */
+typedef struct CUstream_st* fdr_stream_t;
+
+typedef enum fdr_status {
+  FDR_OK = 0,
+  FDR_ERR_INVALID_ARGUMENT = 1,   /* @assert / error() in the reference */
+  FDR_ERR_UNSUPPORTED_SIZE = 2,   /* FFT length with a prime factor > 64, or beyond limits */
+  FDR_ERR_UNSUPPORTED_WINDOW = 3, /* zdtfdr.jl:311-313 "unsupported window type" */
+  FDR_ERR_OUT_OF_MEMORY = 4,
+  FDR_ERR_CUDA = 5,               /* a CUDA runtime call failed */
+  FDR_ERR_CAPACITY = 6,           /* more proto-hits than the caller's capacity */
+  FDR_ERR_NO_DEVICE = 7
+} fdr_status;
+
+typedef enum fdr_window {
+  FDR_WINDOW_RECT = 0,    /* zdtfdr.jl:307-309 (default) */
+  FDR_WINDOW_HAMMING = 1, /* zdtfdr.jl:303-305: 0.53836 + 0.46164*cospi(2k/Nf) */
+  FDR_WINDOW_CUSTOM = 2   /* w(k, Nf) evaluated by the caller: K = Nf/2+1 float64 values */
+} fdr_window;
+
+/* Workspace flags (fdr_zdt_create). */
+#define FDR_ZDT_OUTPUT_ALIGNED 0x1u /* accepted for API parity (FFTW planner hint); no effect */
+#define FDR_ZDT_EXACT_PHASE 0x2u    /* staged stages reduce chirp phases exactly (default:
+                                       the reference's Float32 phase arguments) */
+#define FDR_ZDT_STAGED_ONLY 0x4u    /* fdr_zdt_execute always runs the staged kernels */
+
+/* Rate arithmetic for intshift/intfdr (round(rate*(t-1)) in the rate's element type). */
+#define FDR_RATES_F64 0
+#define FDR_RATES_F32 1
+
+/* ---------------------------------------------------------------------------------- */
+/* Library information                                                                 */
+/* ---------------------------------------------------------------------------------- */
+const char* fdr_version(void);
+const char* fdr_last_error_string(void);
+const char* fdr_status_string(int status);
+/* Number of CUDA kernels this library has launched in the process (a diagnostic with no
+   counterpart in the reference; used to count device launches in benchmarks). */
+int64_t fdr_kernel_launches(void);
+/* fdrsynchronize (fdrutils.jl:129-130; CuArray method ext:26-28): synchronise `stream`
+   (NULL: the whole device). */
+int fdr_synchronize(fdr_stream_t stream);
+
+/* ---------------------------------------------------------------------------------- */
+/* zdtutils.jl                                                                         */
+/* ---------------------------------------------------------------------------------- */
+/* calcNl (zdtutils.jl:7-9): smallest n >= Nt+Nr-1 whose prime factors are in `factors`
+   (host array; NULL -> (2,3,5)).  Returns -1 on invalid input. */
+int64_t fdr_calc_nl(int64_t Nt, int64_t Nr, const int64_t* factors, int nfactors);
+/* growNr (zdtutils.jl:17-19). */
+int64_t fdr_grow_nr(int64_t Nt, int64_t Nr, const int64_t* factors, int nfactors);
+/* estimate_memory (zdtutils.jl:35-53): the reference's formula, in bytes. */
+int64_t fdr_estimate_memory(int64_t Nf, int64_t Nt, int64_t Nr, int64_t Ni, int64_t No,
+                            const int64_t* factors, int nfactors);
+
+/* ---------------------------------------------------------------------------------- */
+/* ZDT workspace and stages (zdtfdr.jl)                                                */
+/* ---------------------------------------------------------------------------------- */
+typedef struct fdr_zdt fdr_zdt;
+
+typedef struct fdr_zdt_info {
+  int64_t Nf, Nt, Nr, Nl, K; /* K = Nf/2 + 1 */
+  float r0, dr;
+  uint32_t flags;
+  int32_t fused;             /* 1 if fdr_zdt_execute uses the fused kernels */
+  int64_t bytes;             /* device bytes owned by the workspace */
+  int32_t nfactors;
+  int64_t factors[8];
+} fdr_zdt_info;
+
+/* ZDTWorkspace(spectrogram, r0, dr, Nr, factors; output_aligned) (zdtfdr.jl:37-87 and
+   plan_ffts! ext:50-82): allocates F (K x Nt), Y (K x Nl), V (K x Nl) and FFT scratch,
+   runs input!(spectrogram) when `spectrogram` is non-NULL, computes V (computeV!,
+   zdtfdr.jl:173-187) and synchronises `stream` (zdtfdr.jl:72). */
+int fdr_zdt_create(fdr_zdt** ws, const float* spectrogram, int64_t Nf, int64_t Nt,
+                   float r0, float dr, int64_t Nr, const int64_t* factors, int nfactors,
+                   uint32_t flags, fdr_stream_t stream);
+int fdr_zdt_destroy(fdr_zdt* ws);
+/* show / sizeof / driftrates (zdtfdr.jl:89-103, zdtutils.jl:62-64). */
+int fdr_zdt_get_info(const fdr_zdt* ws, fdr_zdt_info* info);
+/* Field access to ws.F, ws.Y (Yf and Ys are its first Nt / Nr columns) and ws.V. */
+int fdr_zdt_buffers(fdr_zdt* ws, void** F, void** Y, void** V);
+/* input! (zdtfdr.jl:209-212): F = rfft(spectrogram, dims=1). */
+int fdr_zdt_input(fdr_zdt* ws, const float* spectrogram, fdr_stream_t stream);
+/* preprocess! (zdtfdr.jl:221-239): Yf = F .* prephase(r0); Y[:, Nt+1:end] = 0. */
+int fdr_zdt_preprocess(fdr_zdt* ws, float r0, fdr_stream_t stream);
+/* convolve! (zdtfdr.jl:249-253): Y = ifft_l(fft_l(Y) .* V) (normalised). */
+int fdr_zdt_convolve(fdr_zdt* ws, fdr_stream_t stream);
+/* postprocess! (zdtfdr.jl:297-321): Ys .*= postphase .* w(k, Nf).  `custom_window` is a
+   device array of K float64 values for FDR_WINDOW_CUSTOM, else ignored. */
+int fdr_zdt_postprocess(fdr_zdt* ws, int window, const double* custom_window,
+                        fdr_stream_t stream);
+/* output! (zdtfdr.jl:328-331; CuArray method ext:94-103): dest (Nf x Nr, leading
+   dimension Nf) = irfft(Ys, Nf) (normalised).  Like the reference's CuArray method it may
+   clobber Ys, so call it once per ZDT. */
+int fdr_zdt_output(fdr_zdt* ws, float* dest, fdr_stream_t stream);
+/* zdtfdr!([w,] dests, ws[, spectrogram]; r0) (zdtfdr.jl:349-378): if `spectrogram` is
+   non-NULL runs input!, then for b in 0..nbatch-1 computes the FDR for rates
+   r0s[b] + j*dr (j < Nr) into dests[b] (Nf x Nr).  `r0s` and `dests` are HOST arrays of
+   nbatch entries; r0s == NULL uses the workspace's r0 for every batch.  Uses the fused
+   kernels when available (power-of-two Nf >= 4096 and FDR_ZDT_STAGED_ONLY not set),
+   else the staged stages.  After a fused call the contents of Y are unspecified. */
+int fdr_zdt_execute(fdr_zdt* ws, const float* spectrogram, const float* r0s, int64_t nbatch,
+                    float* const* dests, int window, const double* custom_window,
+                    fdr_stream_t stream);
+/* Per-stage device time of the last fdr_zdt_execute call (enable with
+   fdr_zdt_set_timing(ws, 1)); times[i] in milliseconds, names via stage_names. */
+int fdr_zdt_set_timing(fdr_zdt* ws, int enable);
+int fdr_zdt_stage_times(fdr_zdt* ws, float* times_ms, int max_stages, int* nstages,
+                        const char** stage_names);
+
+/* ---------------------------------------------------------------------------------- */
+/* intfdr.jl                                                                           */
+/* ---------------------------------------------------------------------------------- */
+/* intshift! (intfdr.jl:7-14): dout[:, t] = circshift(din[:, t], -round(rate*t)). */
+int fdr_intshift(const float* din, int64_t Nf, int64_t Nt, double rate, int rate_type,
+                 float* dout, fdr_stream_t stream);
+/* intfdr! (intfdr.jl:34-45): fdr[n, j] = sum over t = 0..Nt-1, in t order from +0.0f, of
+   spec[(n + round(rates[j]*t)) mod Nf, t].  `rates` is a HOST array of Nr values; the
+   product rates[j]*t is formed in float64 (FDR_RATES_F64) or float32 (FDR_RATES_F32) and
+   rounded to nearest, ties to even, as Julia's round does.  Bit-exact with the
+   reference's CPU intfdr. */
+int fdr_intfdr(const float* spec, int64_t Nf, int64_t Nt, const double* rates, int64_t Nr,
+               int rate_type, float* fdr, fdr_stream_t stream);
+/* intfdr! with caller-computed integer shifts: `shifts` is a HOST array of Nr*Nt int64
+   (shift of rate j at time t at shifts[j*Nt + t]). */
+int fdr_intfdr_shifts(const float* spec, int64_t Nf, int64_t Nt, const int64_t* shifts,
+                      int64_t Nr, float* fdr, fdr_stream_t stream);
+
+/* ---------------------------------------------------------------------------------- */
+/* fftfdr.jl                                                                           */
+/* ---------------------------------------------------------------------------------- */
+typedef struct fdr_fft_ws fdr_fft_ws;
+/* fftfdr_workspace(spectrogram) (fftfdr.jl:39-59): holds rfft(spectrogram) (K x Nt). */
+int fdr_fftfdr_workspace(fdr_fft_ws** ws, const float* spectrogram, int64_t Nf, int64_t Nt,
+                         fdr_stream_t stream);
+/* fftfdr_workspace! (fftfdr.jl:69-84): re-FFT a same-size spectrogram into ws. */
+int fdr_fftfdr_workspace_update(fdr_fft_ws* ws, const float* spectrogram, int64_t Nf,
+                                int64_t Nt, fdr_stream_t stream);
+int fdr_fftfdr_destroy(fdr_fft_ws* ws);
+/* Device pointer of ws.dest_rfft (K x Nt complex). */
+int fdr_fftfdr_rfft_buffer(fdr_fft_ws* ws, void** F);
+/* fdshiftsum! (fftfdr.jl:86-96): dest (Nf) = irfft(sum_t F .* phasor(rate)). */
+int fdr_fdshiftsum(fdr_fft_ws* ws, float rate, float* dest, fdr_stream_t stream);
+/* fdshift! (fftfdr.jl:104-111): de-Dopplered spectrogram dest (Nf x Nt). */
+int fdr_fdshift(fdr_fft_ws* ws, float rate, float* dest, fdr_stream_t stream);
+/* fftfdr! (fftfdr.jl:126-134): fdr[:, j] = fdshiftsum(rates[j]) for a HOST array of Nr
+   float32 rates; fdr has leading dimension Nf. */
+int fdr_fftfdr(fdr_fft_ws* ws, const float* rates, int64_t Nr, float* fdr,
+               fdr_stream_t stream);
+
+/* ---------------------------------------------------------------------------------- */
+/* fdrutils.jl                                                                         */
+/* ---------------------------------------------------------------------------------- */
+/* fdrstats (fdrutils.jl:39-50) over nb matrices (HOST array of nb device pointers), each
+   Nf x Nrb with leading dimension Nf: m = mean of column 1 of the first matrix,
+   s = minimum over all columns of the corrected standard deviation.  Accumulates in
+   float64.  Synchronises `stream` and writes host doubles. */
+int fdr_stats(const float* const* fdrs, int64_t nb, int64_t Nf, int64_t Nrb, double* m,
+              double* s, fdr_stream_t stream);
+/* fdrnormalize! (fdrutils.jl:70-90): x = (x - m) / s in float32 for nb matrices. */
+int fdr_normalize(float* const* fdrs, int64_t nb, int64_t Nf, int64_t Nrb, float m, float s,
+                  fdr_stream_t stream);
+/* findprotohits (fdrutils.jl:148-169) over nb matrices treated as hcat'd: every (i, j)
+   with fdr[i, j] >= threshold, in column-major (findall) order, written as ZERO-based
+   int64 pairs hits[2*h] = i, hits[2*h+1] = j (device buffer of 2*capacity int64).
+   Each float32 element is compared with the float64 threshold (Julia promotes the
+   Float32 element for `>=(threshold)` with a Float64 threshold).  snr != 0 replaces
+   `threshold` by fdrdenormalize(threshold, fdrs) = threshold*s + m, formed in float64
+   from the float32-rounded m and s.  Synchronises `stream`; *count (host) receives the
+   total number of hits; if it exceeds `capacity`, the first `capacity` hits are written
+   and FDR_ERR_CAPACITY is returned.  *threshold_used (host, may be NULL) receives the
+   threshold compared against. */
+int fdr_findprotohits(const float* const* fdrs, int64_t nb, int64_t Nf, int64_t Nrb,
+                      double threshold, int snr, int64_t* hits, int64_t capacity,
+                      int64_t* count, double* threshold_used, fdr_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FDR_B200_H */

@@ -1,0 +1,73 @@
+"""CPU tests of the C-ABI library and the host-side logic (no kernels launched)."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "fdr_b200.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(fdr_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_loads_and_exports_every_declared_symbol(fdr):
+    lib = fdr._lib.lib()
+    names = declared_functions()
+    assert len(names) >= 30
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    # every declared entry point has a ctypes signature in the binding
+    assert set(names) <= set(fdr._lib.SIGNATURES), set(names) - set(fdr._lib.SIGNATURES)
+
+
+def test_version_and_status_strings(fdr):
+    lib = fdr._lib.lib()
+    assert b"sm_100a" in lib.fdr_version()
+    assert lib.fdr_status_string(0) == b"FDR_OK"
+    assert lib.fdr_status_string(6) == b"FDR_ERR_CAPACITY"
+
+
+def test_zdtutils_via_abi(fdr, oracle):
+    for Nt, Nr in [(16, 129), (16, 33), (2, 3), (64, 257), (32, 65), (16, 1)]:
+        assert fdr.calcNl(Nt, Nr) == oracle.calcNl(Nt, Nr)
+        assert fdr.growNr(Nt, Nr) == oracle.growNr(Nt, Nr)
+    assert fdr.calcNl(16, 129, (2,)) == 256
+    assert fdr.calcNl(16, 129, (2, 3, 5, 7)) == oracle.calcNl(16, 129, (2, 3, 5, 7))
+    assert fdr.estimate_memory(2 ** 20, 16, 129, 2, 3) == oracle.estimate_memory(2 ** 20, 16, 129, 2, 3)
+    with pytest.raises(ValueError):
+        fdr.calcNl(16, 129, (1,))
+
+
+def test_argument_errors_without_device(fdr):
+    lib = fdr._lib.lib()
+    h = C.c_void_p()
+    st = lib.fdr_zdt_create(C.byref(h), None, 0, 16, 0.0, 1.0, 10, None, 0, 0, None)
+    assert st == fdr._lib.FDR_ERR_INVALID_ARGUMENT
+    assert b"bad sizes" in lib.fdr_last_error_string()
+    st = lib.fdr_zdt_create(C.byref(h), None, 67 * 2, 16, 0.0, 1.0, 10, None, 0, 0, None)
+    assert st == fdr._lib.FDR_ERR_UNSUPPORTED_SIZE
+    st = lib.fdr_intfdr(None, 10, 2, None, 1, 0, None, None)
+    assert st == fdr._lib.FDR_ERR_INVALID_ARGUMENT
+    cnt = C.c_int64()
+    st = lib.fdr_findprotohits(None, 1, 10, 2, 1.0, 0, None, 0, C.byref(cnt), None, None)
+    assert st == fdr._lib.FDR_ERR_INVALID_ARGUMENT
+
+
+def test_batchrates_host_matches_oracle(fdr, oracle):
+    for args in [(16, 1.0, -4.0, None, 360), (16, 0.5, 10.0, -3.0, 50),
+                 (32, -0.25, -2.0, 5.0, 40), (17, 0.1, -100.0, 100.0, 360), (64, 1.0, -8.0, 8.0, 100)]:
+        Nt, dh, r1, r2, Nrb = args
+        mine = fdr.batchrates(Nt, dh, r1, r2, Nrb=Nrb)
+        ref = oracle.batchrates(Nt, dh, r1, r2, Nrb=Nrb)
+        assert [list(b) for b in mine] == ref
+
+
+def test_rate_range_params(fdr):
+    rr = fdr.batchrates(16, 1.0, -4.0)[0]
+    assert rr.first == rr.start and len(rr) == rr.length
+    assert list(rr)[1] - list(rr)[0] == rr.step

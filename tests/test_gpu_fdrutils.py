@@ -1,0 +1,71 @@
+"""GPU tests of fdrstats / fdrnormalize! / findprotohits (fdrutils.jl)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def _fdr(oracle, Nf=65536, Nr=33, seed=1):
+    spec, _ = oracle.synth_spectrogram(Nf, 16, 3, 20, 20, 4, seed=seed)
+    return oracle.intfdr(spec, [-4.0 + 0.25 * j for j in range(Nr)])
+
+
+def test_stats(fdr, oracle):
+    a = _fdr(oracle)
+    m, s = fdr.fdrstats(fdr.as_device_f32(a))
+    mr, sr = oracle.fdrstats(a)
+    assert abs(m - mr) <= 1e-6 * abs(mr) and abs(s - sr) <= 1e-6 * sr
+    b = _fdr(oracle, seed=2)
+    m2, s2 = fdr.fdrstats([fdr.as_device_f32(a), fdr.as_device_f32(b)])
+    mr2, sr2 = oracle.fdrstats([a, b])
+    assert abs(m2 - mr2) <= 1e-6 * abs(mr2) and abs(s2 - sr2) <= 1e-6 * sr2
+
+
+def test_normalize_bit_exact(fdr, oracle):
+    a = _fdr(oracle)
+    m, s = np.float32(16.25), np.float32(3.75)
+    g = fdr.as_device_f32(a.copy())
+    fdr.fdrnormalize_(g, m, s)
+    ref = oracle.fdrnormalize(a, m, s)
+    assert np.array_equal(g.cpu().numpy().view(np.uint32), ref.view(np.uint32))
+    assert fdr.fdrnormalize(20.0, 16.0, 2.0) == 2.0
+    assert fdr.fdrdenormalize(10, 16.0, 2.0) == 36.0
+
+
+@pytest.mark.parametrize("thr", [30.0, 45.5, 1e9])
+def test_findprotohits_exact(fdr, oracle, thr):
+    a = _fdr(oracle)
+    hits = fdr.findprotohits(fdr.as_device_f32(a), thr)
+    ref = oracle.findprotohits(a, thr)
+    assert np.array_equal(hits, ref)
+
+
+def test_findprotohits_snr_and_batches(fdr, oracle):
+    a, b = _fdr(oracle, seed=3), _fdr(oracle, seed=4)
+    ga, gb = fdr.as_device_f32(a), fdr.as_device_f32(b)
+    hits, thr = fdr.findprotohits([ga, gb], 8.0, snr=True, return_threshold=True)
+    mr, sr = oracle.fdrstats([a, b])
+    thr_ref = 8.0 * float(np.float32(sr)) + float(np.float32(mr))
+    assert abs(thr - thr_ref) <= 1e-6 * thr_ref
+    ref = oracle.findprotohits([a, b], thr)
+    assert np.array_equal(hits, ref)
+    assert hits[:, 1].max() >= a.shape[1]  # offsets of the second matrix
+
+
+def test_findprotohits_capacity(fdr, oracle):
+    a = _fdr(oracle, Nf=4096, Nr=5)
+    g = fdr.as_device_f32(a)
+    lib = fdr._lib.lib()
+    buf = torch.empty((4, 2), dtype=torch.int64, device="cuda")
+    cnt = C.c_int64()
+    ptrs = (C.c_void_p * 1)(g.data_ptr())
+    st = lib.fdr_findprotohits(ptrs, 1, 4096, 5, 0.0, 0, C.c_void_p(buf.data_ptr()), 4,
+                               C.byref(cnt), None, None)
+    assert st == fdr._lib.FDR_ERR_CAPACITY and cnt.value == 4096 * 5
+    ref = oracle.findprotohits(a, 0.0)
+    assert np.array_equal(buf.cpu().numpy(), ref[:4])
+    # the Python wrapper grows its buffer and retries
+    assert len(fdr.findprotohits(g, 0.0, capacity=16)) == 4096 * 5

@@ -1,0 +1,127 @@
+"""CPU tests of the oracle itself: pinned to the reference's known answers
+(test/runtests.jl:5-32) and cross-checked between its FP32 mirror and FP64 tiers."""
+from fractions import Fraction
+
+import numpy as np
+import pytest
+
+
+def test_known_answers_intshift_intfdr(oracle, golden):
+    d = np.array(golden["spectrogram"], dtype=np.float32)
+    assert np.array_equal(oracle.intshift(d, golden["intshift_rate"]),
+                          np.array(golden["intshift_expected"], dtype=np.float32))
+    # runtests.jl:20 compares with `==`
+    assert np.array_equal(oracle.intfdr(d, golden["rates"]),
+                          np.array(golden["fdr_expected"], dtype=np.float32))
+
+
+def test_known_answers_fftfdr(oracle, golden):
+    d = np.array(golden["spectrogram"], dtype=np.float32)
+    ws = oracle.fftfdr_workspace(d)
+    np.testing.assert_allclose(oracle.fdshift(ws, 1), np.array(golden["intshift_expected"]),
+                               atol=1e-6)
+    np.testing.assert_allclose(oracle.fftfdr(ws, golden["rates"]),
+                               np.array(golden["fdr_expected"]), atol=1e-6)
+
+
+def test_known_answers_zdtfdr(oracle, golden):
+    d = np.array(golden["spectrogram"], dtype=np.float32)
+    ws = oracle.ZDTWorkspace(d, -1, 1, 3)
+    assert ws.Nl == 4  # nextprod((2,3,5), 2+3-1)
+    np.testing.assert_allclose(ws.zdtfdr(), np.array(golden["fdr_expected"]), atol=1e-6)
+
+
+def test_truth_known_answers(oracle, golden):
+    d = np.array(golden["spectrogram"], dtype=np.float32)
+    np.testing.assert_allclose(oracle.fdr_truth(d, [-1.0, 0.0, 1.0]),
+                               np.array(golden["fdr_expected"]), atol=1e-12)
+
+
+def test_truth_equals_circular_shift_at_integer_rates(oracle):
+    spec, _ = oracle.synth_spectrogram(1024, 8, 2, 20, 20, 3, seed=1)
+    rates = [-3.0, -1.0, 0.0, 2.0, 3.0]
+    shifts = [[int(r * t) for t in range(8)] for r in rates]
+    np.testing.assert_allclose(oracle.fdr_truth(spec, rates), oracle.intfdr_f64(spec, shifts),
+                               rtol=0, atol=1e-9)
+
+
+@pytest.mark.parametrize("Nf,Nt,r0,dr,Nr", [(4096, 16, -4.0, 0.25, 33), (1000, 7, 2.0, -0.5, 9),
+                                           (375, 5, -1.0, 0.125, 17)])
+def test_fp32_zdt_mirror_vs_fp64_truth(oracle, Nf, Nt, r0, dr, Nr):
+    spec, _ = oracle.synth_spectrogram(Nf, Nt, 3, 20, 20, 4, seed=Nf)
+    out = oracle.zdtfdr(spec, r0, dr, Nr)
+    truth = oracle.fdr_truth(spec, [r0 + j * dr for j in range(Nr)])
+    assert oracle.rel_linf(out, truth) < 1e-5
+
+
+def test_fp32_fftfdr_mirror_vs_fp64_truth(oracle):
+    spec, _ = oracle.synth_spectrogram(2048, 16, 2, 20, 20, 4, seed=3)
+    rates = [-4.0 + 0.25 * j for j in range(33)]
+    ws = oracle.fftfdr_workspace(spec)
+    assert oracle.rel_linf(oracle.fftfdr(ws, rates), oracle.fdr_truth(spec, rates)) < 1e-5
+
+
+def test_zdt_equals_intfdr_at_integer_rates(oracle):
+    spec, _ = oracle.synth_spectrogram(2048, 16, 3, 20, 20, 3, seed=5)
+    out = oracle.zdtfdr(spec, -3.0, 1.0, 7)
+    ref = oracle.intfdr(spec, [-3, -2, -1, 0, 1, 2, 3])
+    assert oracle.rel_linf(out, ref) < 1e-5
+
+
+def test_windows_mirror(oracle):
+    spec, _ = oracle.synth_spectrogram(512, 8, 1, 20, 20, 2, seed=9)
+    ws = oracle.ZDTWorkspace(spec, -2.0, 0.5, 9)
+    rect = ws.zdtfdr(window="rect")
+    ham = ws.zdtfdr(window="hamming")
+    same = ws.zdtfdr(window=lambda n, N: 1.0)
+    np.testing.assert_allclose(same, rect, atol=1e-5 * np.abs(rect).max())
+    assert not np.allclose(ham, rect)
+    with pytest.raises(ValueError):
+        ws.zdtfdr(window="blackman")
+
+
+def test_heavytest_standin_peak(oracle):
+    """Stand-in for test/heavytests.jl:9-40 (Voyager-1 data unavailable): a tone starting at
+    channel 54 (0-based) drifting -2.5 ch/step, rates 0:-0.25:-5 -> peak at (54, 10)."""
+    rng = np.random.Generator(np.random.PCG64(11))
+    Nf, Nt = 150, 16
+    spec = rng.exponential(1.0, size=(Nf, Nt)).astype(np.float32)
+    for t in range(Nt):
+        c = 54 - 2.5 * t
+        lo = int(np.floor(c))
+        f = c - lo
+        spec[lo % Nf, t] += 40 * (1 - f)
+        spec[(lo + 1) % Nf, t] += 40 * f
+    rates = [0.0 - 0.25 * j for j in range(21)]
+    for out in (oracle.intfdr(spec, rates),
+                oracle.fftfdr(oracle.fftfdr_workspace(spec), rates),
+                oracle.zdtfdr(spec, 0.0, -0.25, 21)):
+        assert np.unravel_index(np.argmax(out), out.shape) == (54, 10)
+
+
+def test_zdtutils(oracle):
+    assert oracle.calcNl(16, 129) == 144
+    assert oracle.calcNl(16, 33) == 48
+    assert oracle.calcNl(2, 3) == 4
+    assert oracle.growNr(16, 129) == 129
+    assert oracle.growNr(16, 30) == 30
+    assert oracle.calcNl(16, 129, (2,)) == 256
+    assert oracle.estimate_memory(2 ** 20, 16, 129) == 4 * (2 ** 20 * 16 * 4 + 2 ** 20 * 144 * 3
+                                                          + 2 ** 20 * 129)
+
+
+def test_batchrates_properties(oracle):
+    for Nt, dh, r1, r2, Nrb in [(16, 1.0, -4.0, None, 360), (16, 0.5, 10.0, -3.0, 50),
+                                (32, -0.25, -2.0, 5.0, 40), (17, 0.1, -100.0, 100.0, 360)]:
+        batches = oracle.batchrates(Nt, dh, r1, r2, Nrb=Nrb)
+        n = len(batches[0])
+        assert all(len(b) == n for b in batches)
+        assert oracle.growNr(Nt, n) == n
+        flat = [r for b in batches for r in b]
+        steps = {flat[i + 1] - flat[i] for i in range(len(flat) - 1)}
+        assert steps <= {Fraction(1, Nt - 1), Fraction(-1, Nt - 1)}
+        lo, hi = (r1, -r1 if r2 is None else r2)
+        lo, hi = min(lo, hi), max(lo, hi)
+        span = {round(lo / dh), round(hi / dh)}
+        covered = {int(r * (Nt - 1)) for r in flat}
+        assert span <= covered
