@@ -5,6 +5,7 @@
 #include <map>
 #include <mutex>
 
+#include "fft_device.cuh"
 #include "fft_engine.cuh"
 
 namespace fdr {
@@ -56,90 +57,6 @@ __device__ __forceinline__ float2 root_at(const float2* roots, int m, int sign) 
   float2 w = __ldg(roots + m);
   return sign > 0 ? cconj(w) : w;
 }
-
-template <int R>
-struct Dft;
-
-template <>
-struct Dft<2> {
-  __device__ __forceinline__ static void run(float2* v, int) {
-    float2 a = v[0], b = v[1];
-    v[0] = cadd(a, b);
-    v[1] = csub(a, b);
-  }
-};
-
-template <>
-struct Dft<4> {
-  __device__ __forceinline__ static void run(float2* v, int sign) {
-    float2 a = cadd(v[0], v[2]), b = csub(v[0], v[2]);
-    float2 c = cadd(v[1], v[3]), d = csub(v[1], v[3]);
-    float2 di = cmul_i(d, sign);  // sign*i*d
-    v[0] = cadd(a, c);
-    v[2] = csub(a, c);
-    v[1] = cadd(b, di);
-    v[3] = csub(b, di);
-  }
-};
-
-template <>
-struct Dft<8> {
-  __device__ __forceinline__ static void run(float2* v, int sign) {
-    const float h = 0.70710678118654752440f;
-    float2 a[4], b[4];
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      a[r] = cadd(v[r], v[r + 4]);
-      b[r] = csub(v[r], v[r + 4]);
-    }
-    // b[r] *= exp(sign*2*pi*i*r/8)
-    float s = (float)sign;
-    b[1] = make_float2(h * (b[1].x - s * b[1].y), h * (b[1].y + s * b[1].x));
-    b[2] = cmul_i(b[2], sign);
-    b[3] = make_float2(h * (-b[3].x - s * b[3].y), h * (-b[3].y + s * b[3].x));
-    Dft<4>::run(a, sign);
-    Dft<4>::run(b, sign);
-#pragma unroll
-    for (int m = 0; m < 4; ++m) {
-      v[2 * m] = a[m];
-      v[2 * m + 1] = b[m];
-    }
-  }
-};
-
-template <>
-struct Dft<3> {
-  __device__ __forceinline__ static void run(float2* v, int sign) {
-    const float c = -0.5f, sn = 0.86602540378443864676f;
-    float2 t1 = cadd(v[1], v[2]);
-    float2 t2 = make_float2(v[0].x + c * t1.x, v[0].y + c * t1.y);
-    float2 d = csub(v[1], v[2]);
-    float2 t3 = cmul_i(cscale(d, sn), sign);
-    v[0] = cadd(v[0], t1);
-    v[1] = cadd(t2, t3);
-    v[2] = csub(t2, t3);
-  }
-};
-
-template <>
-struct Dft<5> {
-  __device__ __forceinline__ static void run(float2* v, int sign) {
-    const float c1 = 0.30901699437494742410f, c2 = -0.80901699437494742410f;
-    const float s1 = 0.95105651629515357212f, s2 = 0.58778525229247312917f;
-    float2 t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
-    float2 t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
-    float2 v0 = v[0];
-    float2 a1 = make_float2(v0.x + c1 * t1.x + c2 * t2.x, v0.y + c1 * t1.y + c2 * t2.y);
-    float2 a2 = make_float2(v0.x + c2 * t1.x + c1 * t2.x, v0.y + c2 * t1.y + c1 * t2.y);
-    float2 b1 = cmul_i(make_float2(s1 * t3.x + s2 * t4.x, s1 * t3.y + s2 * t4.y), sign);
-    float2 b2 = cmul_i(make_float2(s2 * t3.x - s1 * t4.x, s2 * t3.y - s1 * t4.y), sign);
-    v[0] = cadd(v0, cadd(t1, t2));
-    v[1] = cadd(a1, b1);
-    v[4] = csub(a1, b1);
-    v[2] = cadd(a2, b2);
-    v[3] = csub(a2, b2);
-  }
-};
 
 // One Stockham stage of radix R over bpc transforms of length L held in shared memory.
 template <int R>

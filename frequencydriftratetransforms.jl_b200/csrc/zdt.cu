@@ -194,6 +194,20 @@ static int zdt_compute_V(fdr_zdt* ws, cudaStream_t s) {
   return fft_strided_inplace(ws->V, ws->Nl, ws->K, ws->K, 1, -1, 1.f, nullptr, s);
 }
 
+// One staged ZDT (zdtfdr.jl:355-358) for a given r0 into dest.
+int zdt_staged_run(fdr_zdt* ws, float r0, float* dest, int window, const double* wk,
+                   cudaStream_t s) {
+  FDR_TRY(zdt_preprocess(ws, r0, s));
+  zdt_mark(ws, "preprocess", s);
+  FDR_TRY(zdt_convolve(ws, s));
+  zdt_mark(ws, "convolve", s);
+  FDR_TRY(zdt_postprocess(ws, window, wk, s));
+  zdt_mark(ws, "postprocess", s);
+  FDR_TRY(zdt_output(ws, dest, s));
+  zdt_mark(ws, "output", s);
+  return FDR_OK;
+}
+
 static bool fft_len_ok(long long N) {
   int radix[kMaxStages], nst;
   if (N <= kMaxCtaElems) return plan_radices(N, radix, &nst);
@@ -375,14 +389,7 @@ int fdr_zdt_execute(fdr_zdt* ws, const float* spectrogram, const float* r0s, int
     if (use_fused) {
       FDR_TRY(zdt_fused_run(ws, r0, dests[b], window, custom_window, s));
     } else {
-      FDR_TRY(zdt_preprocess(ws, r0, s));
-      zdt_mark(ws, "preprocess", s);
-      FDR_TRY(zdt_convolve(ws, s));
-      zdt_mark(ws, "convolve", s);
-      FDR_TRY(zdt_postprocess(ws, window, custom_window, s));
-      zdt_mark(ws, "postprocess", s);
-      FDR_TRY(zdt_output(ws, dests[b], s));
-      zdt_mark(ws, "output", s);
+      FDR_TRY(zdt_staged_run(ws, r0, dests[b], window, custom_window, s));
     }
   }
   return FDR_OK;

@@ -1,15 +1,620 @@
-// Fused ZDT path for power-of-two Nf (placeholder: not yet enabled).
+// Fused ZDT path for power-of-two Nf (2^12 .. 2^22) and Nt <= 16.
+//
+// The reference computes zdtfdr! as rfft -> prephase -> FFT_l -> .*V -> IFFT_l ->
+// postphase -> irfft (zdtfdr.jl:349-362), materialising F, Y (K x Nl) and V (K x Nl) in
+// device memory.  Mathematically the chirp-Z stage evaluates, for every frequency bin k
+// and drift rate r_j = r0 + j*dr,
+//     S_j[k] = sum_t F[k, t] * exp(2*pi*i * k * t * r_j / Nf)
+// (the fftfdr.jl phasor form; Bluestein's convolution computes exactly this).  For the
+// small Nt of this path the direct evaluation per bin (Horner's rule in t) costs about
+// the same arithmetic as three length-Nl FFTs and needs neither V nor Y, so this path
+// keeps F on chip and never writes the K x Nl intermediates:
+//
+//   kernel A (zdtf_input):  four-step pass 1 of the forward FFT of two real columns packed
+//                           as one complex column (t pairs): DFT_P over n_b, twiddle.
+//   kernel B (zdtf_czt):    per pair of bin residues {k1, P-k1}: forward DFT_Q (pass 2) and
+//                           two-for-one unpack into F[k, t] held in registers; then, per
+//                           block of drift rates, S_j[k] by Horner's rule with exact
+//                           integer phase reduction, the window, two-for-one packing of
+//                           rate pairs, inverse DFT_Q (pass 1 of the output FFT) and the
+//                           inter-pass twiddle (with the 1/Nf scale).
+//   kernel C (zdtf_output): inverse DFT_P (pass 2), real/imaginary parts to the two
+//                           output columns of each rate pair.
+//
+// Nf = P*Q; bin k = k1 + P*k2, channel n = na + Q*nb.  Phases: r0 and dr are float32,
+// hence dyadic, so k*r_j/Nf is an exact fraction m / 2^bits with m computed in 64-bit
+// integer arithmetic modulo 2^bits; only the final conversion to a float in [-1, 1)
+// half-turns rounds.
+#include <math.h>
+#include <string.h>
+
+#include "fft_device.cuh"
+#include "fft_engine.cuh"
 #include "zdt_ws.cuh"
 
 namespace fdr {
 
-bool zdt_fused_eligible(int64_t, int64_t, int64_t) { return false; }
-int zdt_fused_setup(fdr_zdt*) { return FDR_OK; }
-int zdt_fused_input(fdr_zdt*, const float*, cudaStream_t) { return FDR_ERR_INVALID_ARGUMENT; }
-int zdt_fused_A_to_F(fdr_zdt*, cudaStream_t) { return FDR_ERR_INVALID_ARGUMENT; }
-int zdt_fused_run(fdr_zdt*, float, float*, int, const double*, cudaStream_t) {
-  return FDR_ERR_INVALID_ARGUMENT;
+constexpr int kFusedMinLog2 = 12;
+constexpr int kFusedMaxLog2 = 22;
+constexpr int kFusedMaxNt = 16;
+constexpr int kRatesPerBlock = 4;  // 2 rate pairs per inverse-FFT block in kernel B
+
+struct PhaseInt {
+  unsigned long long R0, Rd, mask;
+  int bits;
+  float scale;  // 2^(1-bits): converts a signed residue to half-turns
+};
+
+struct FusedTables {
+  const float2* rootsP;  // exp(-2 pi i m / P), m < P
+  const float2* rootsQ;  // exp(-2 pi i m / Q), m < Q
+  const float2* tw_lo;   // exp(-2 pi i m / N), m < 2^B
+  const float2* tw_hi;   // exp(-2 pi i m 2^B / N), m < N / 2^B
+  int B;
+};
+
+// exp(-2 pi i m / N) for 0 <= m < N (two-level table product).
+__device__ __forceinline__ float2 tw_fwd(const FusedTables& t, long long m) {
+  return cmul(__ldg(t.tw_hi + (m >> t.B)), __ldg(t.tw_lo + (m & ((1LL << t.B) - 1))));
 }
-void zdt_fused_release(fdr_zdt*) {}
+
+// exp(2 pi i ph / 2^bits) for a residue 0 <= ph < 2^bits.
+__device__ __forceinline__ float2 cis_phase(unsigned long long ph, const PhaseInt& p) {
+  long long sp = (long long)ph;
+  if ((ph >> (p.bits - 1)) & 1ULL) sp -= (long long)(1ULL << p.bits);
+  return cispif(__ll2float_rn(sp) * p.scale);
+}
+
+// ------------------------------------------------------------------------------------
+// Kernel A: forward four-step pass 1.  grid (Q/TA, NP); A[p][k1][na].
+// ------------------------------------------------------------------------------------
+template <int P, int TA, int T>
+__global__ void __launch_bounds__(T)
+zdtf_input_kernel(const float* __restrict__ spec, long long N, int Nt, int Q,
+                  float2* __restrict__ A, FusedTables tab) {
+  constexpr int SS = P + 1;
+  extern __shared__ float2 sm[];
+  float2* buf = sm;
+  float2* roots = sm + TA * SS;
+  const int na0 = blockIdx.x * TA;
+  const int p = blockIdx.y;
+  for (int i = threadIdx.x; i < P; i += T) roots[i] = __ldg(tab.rootsP + i);
+  const float* c0 = spec + (long long)(2 * p) * N;
+  const bool has1 = (2 * p + 1) < Nt;
+  const float* c1 = spec + (long long)(2 * p + 1) * N;
+  for (int e = threadIdx.x; e < TA * P; e += T) {
+    const int seq = e % TA, nb = e / TA;
+    const long long n = (long long)(na0 + seq) + (long long)Q * nb;
+    const float a = __ldcs(c0 + n);
+    const float b = has1 ? __ldcs(c1 + n) : 0.f;
+    buf[seq * SS + nb] = make_float2(a, b);
+  }
+  __syncthreads();
+  smem_fft<P, TA, SS, T, -1>(buf, roots);
+  for (int e = threadIdx.x; e < TA * P; e += T) {
+    const int seq = e % TA, k1 = e / TA;
+    const int na = na0 + seq;
+    const float2 w = tw_fwd(tab, (long long)k1 * na);
+    A[((long long)p * P + k1) * Q + na] = cmul(buf[seq * SS + k1], w);
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// Kernel B helpers
+// ------------------------------------------------------------------------------------
+struct CztArgs {
+  const float2* A;
+  float2* W;          // [pair][k1][na] for pairs [0, npairs)
+  float2* F;          // A->F mode output (K x Nt) or NULL
+  const double* wk;   // custom window values (K) or NULL
+  long long N;
+  int P, Nt, NP, Nr, npairs, pairs_per_group, window;
+  PhaseInt ph;
+  FusedTables tab;
+};
+
+// Position (side, k2) of the bin N - k for the base at (side, k2) of CTA c.
+__device__ __forceinline__ void mirror_of(int c, int side, int k2, int Q, int* ms, int* mk2) {
+  if (c == 0 && side == 0) { *ms = 0; *mk2 = (Q - k2) & (Q - 1); }
+  else if (c == 0) { *ms = 1; *mk2 = Q - 1 - k2; }
+  else { *ms = 1 - side; *mk2 = Q - 1 - k2; }
+}
+
+// Forward pass 2 + two-for-one unpack: G[b][t] = F[k_b, t] for the two bases of this
+// thread (b = side, k2 = threadIdx.x); CTA 0's thread 0 also stores the Nyquist bin's
+// F[N/2, t] into gnyq (shared memory).  buf holds 4 sequences of stride Q+1.
+template <int Q, int NTR>
+__device__ __forceinline__ void czt_forward(const CztArgs& a, int c, const int* k1s, float2* buf,
+                                            const float2* roots, float2* gnyq,
+                                            float2 (&G)[2][NTR]) {
+  constexpr int T = Q / 2;
+  constexpr int SS = Q + 1;
+  const int tid = threadIdx.x;
+#pragma unroll
+  for (int b = 0; b < 2; ++b)
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) G[b][t] = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int p0 = 0; p0 < NTR / 2; p0 += 2) {
+    if (p0 < a.NP) {
+      __syncthreads();
+      for (int e = tid; e < 4 * Q; e += T) {
+        const int seq = e / Q, na = e - seq * Q;
+        const int pp = p0 + (seq >> 1), side = seq & 1;
+        float2 v = make_float2(0.f, 0.f);
+        if (pp < a.NP) v = a.A[((long long)pp * a.P + k1s[side]) * Q + na];
+        buf[seq * SS + na] = v;
+      }
+      __syncthreads();
+      smem_fft<Q, 4, SS, T, -1>(buf, roots);
+#pragma unroll
+      for (int b = 0; b < 2; ++b) {
+        int ms, mk2;
+        mirror_of(c, b, tid, Q, &ms, &mk2);
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const float2 zk = buf[(2 * u + b) * SS + tid];
+          const float2 zm = cconj(buf[(2 * u + ms) * SS + mk2]);
+          const float2 s = cadd(zk, zm), d = csub(zk, zm);
+          G[b][2 * (p0 + u)] = make_float2(0.5f * s.x, 0.5f * s.y);
+          G[b][2 * (p0 + u) + 1] = make_float2(0.5f * d.y, -0.5f * d.x);
+        }
+      }
+      if (c == 0 && tid == 0) {
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const float2 z = buf[(2 * u) * SS + Q / 2];
+          gnyq[2 * (p0 + u)] = make_float2(z.x, 0.f);
+          gnyq[2 * (p0 + u) + 1] = make_float2(z.y, 0.f);
+        }
+      }
+    }
+  }
+  __syncthreads();
+}
+
+template <int NTR>
+__device__ __forceinline__ float2 horner(const float2 (&G)[NTR], float2 w) {
+  float2 s = G[NTR - 1];
+#pragma unroll
+  for (int t = NTR - 2; t >= 0; --t) {
+    s = make_float2(fmaf(s.x, w.x, fmaf(-s.y, w.y, G[t].x)), fmaf(s.x, w.y, fmaf(s.y, w.x, G[t].y)));
+  }
+  return s;
+}
+
+__device__ __forceinline__ float window_value(const CztArgs& a, long long k) {
+  if (a.window == FDR_WINDOW_HAMMING) return (float)(0.53836 + 0.46164 * cospi(2.0 * (double)k / (double)a.N));
+  if (a.window == FDR_WINDOW_CUSTOM) return (float)a.wk[k];
+  return 1.f;
+}
+
+// ------------------------------------------------------------------------------------
+// Kernel B: grid (P/2, rate groups), Q/2 threads.
+// ------------------------------------------------------------------------------------
+template <int Q, int NTR>
+__global__ void __launch_bounds__(Q / 2, 1) zdtf_czt_kernel(CztArgs a) {
+  constexpr int T = Q / 2;
+  constexpr int SS = Q + 1;
+  extern __shared__ float2 sm[];
+  float2* buf = sm;                // 4 * SS
+  float2* roots = buf + 4 * SS;    // Q
+  float2* twr = roots + Q;         // 2 * Q
+  float2* gnyq = twr + 2 * Q;      // NTR
+  const int tid = threadIdx.x;
+  const int c = blockIdx.x;
+  const int P = a.P;
+  const int k1s[2] = {c == 0 ? 0 : c, c == 0 ? P / 2 : P - c};
+  const float invN = 1.0f / (float)a.N;
+  for (int i = tid; i < Q; i += T) roots[i] = __ldg(a.tab.rootsQ + i);
+  for (int i = tid; i < 2 * Q; i += T) {
+    const int side = i / Q, na = i - side * Q;
+    twr[i] = cscale(cconj(tw_fwd(a.tab, (long long)k1s[side] * na)), invN);
+  }
+  float2 G[2][NTR];
+  czt_forward<Q, NTR>(a, c, k1s, buf, roots, gnyq, G);
+
+  // Per-base phase state: w_{k,j} = exp(2 pi i (alpha + j*beta) / 2^bits)
+  const unsigned long long mask = a.ph.mask;
+  unsigned long long alpha[2], beta[2];
+  float2 pw[2][kRatesPerBlock];
+  float win[2];
+#pragma unroll
+  for (int b = 0; b < 2; ++b) {
+    const unsigned long long k = (unsigned long long)k1s[b] + (unsigned long long)P * tid;
+    alpha[b] = (k * a.ph.R0) & mask;
+    beta[b] = (k * a.ph.Rd) & mask;
+#pragma unroll
+    for (int i = 0; i < kRatesPerBlock; ++i) pw[b][i] = cis_phase(((unsigned long long)i * beta[b]) & mask, a.ph);
+    win[b] = window_value(a, (long long)k);
+  }
+  // Nyquist bin (CTA 0, thread 0)
+  const unsigned long long kny = (unsigned long long)(a.N / 2);
+  const unsigned long long alpha_n = (kny * a.ph.R0) & mask, beta_n = (kny * a.ph.Rd) & mask;
+
+  int ms[2], mk2[2];
+#pragma unroll
+  for (int b = 0; b < 2; ++b) mirror_of(c, b, tid, Q, &ms[b], &mk2[b]);
+  const bool dc = (c == 0 && tid == 0);
+
+  const int q_begin = blockIdx.y * a.pairs_per_group;
+  const int q_end = min(a.npairs, q_begin + a.pairs_per_group);
+  for (int q0 = q_begin; q0 < q_end; q0 += kRatesPerBlock / 2) {
+    const int j0 = 2 * q0;
+    float2 S[2][kRatesPerBlock];
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+      const float2 w0 = cis_phase((alpha[b] + (unsigned long long)j0 * beta[b]) & mask, a.ph);
+#pragma unroll
+      for (int jr = 0; jr < kRatesPerBlock; ++jr) {
+        const float2 w = cmul(w0, pw[b][jr]);
+        float2 s = horner<NTR>(G[b], w);
+        if (j0 + jr >= a.Nr) s = make_float2(0.f, 0.f);
+        S[b][jr] = cscale(s, win[b]);
+      }
+    }
+    __syncthreads();  // buf is free
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+#pragma unroll
+      for (int u = 0; u < kRatesPerBlock / 2; ++u) {
+        const float2 sa = S[b][2 * u], sb = S[b][2 * u + 1];
+        if (dc && b == 0) {
+          buf[(2 * u) * SS + 0] = make_float2(sa.x, sb.x);  // real-only DC bin
+        } else {
+          buf[(2 * u + b) * SS + tid] = make_float2(sa.x - sb.y, sa.y + sb.x);       // sa + i sb
+          buf[(2 * u + ms[b]) * SS + mk2[b]] = make_float2(sa.x + sb.y, sb.x - sa.y);  // conj(sa) + i conj(sb)
+        }
+      }
+    }
+    if (c == 0 && tid == 0) {
+      float2 Gn[NTR];
+#pragma unroll
+      for (int t = 0; t < NTR; ++t) Gn[t] = gnyq[t];
+      const float wn = window_value(a, (long long)kny);
+#pragma unroll
+      for (int u = 0; u < kRatesPerBlock / 2; ++u) {
+        float v[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int j = j0 + 2 * u + h;
+          const float2 w = cis_phase((alpha_n + (unsigned long long)j * beta_n) & mask, a.ph);
+          const float2 s = horner<NTR>(Gn, w);
+          v[h] = (j < a.Nr) ? s.x * wn : 0.f;  // real-only Nyquist bin
+        }
+        buf[(2 * u) * SS + Q / 2] = make_float2(v[0], v[1]);
+      }
+    }
+    __syncthreads();
+    smem_fft<Q, kRatesPerBlock, SS, T, +1>(buf, roots);
+    for (int e = tid; e < kRatesPerBlock * Q; e += T) {
+      const int seq = e / Q, na = e - seq * Q;
+      const int q = q0 + (seq >> 1), side = seq & 1;
+      if (q < q_end)
+        a.W[((long long)q * P + k1s[side]) * Q + na] = cmul(buf[seq * SS + na], twr[side * Q + na]);
+    }
+  }
+}
+
+// A -> F (reference layout K x Nt) for the staged stages after a fused input!.
+template <int Q, int NTR>
+__global__ void __launch_bounds__(Q / 2, 1) zdtf_a2f_kernel(CztArgs a) {
+  constexpr int T = Q / 2;
+  constexpr int SS = Q + 1;
+  extern __shared__ float2 sm[];
+  float2* buf = sm;
+  float2* roots = buf + 4 * SS;
+  float2* twr = roots + Q;
+  float2* gnyq = twr + 2 * Q;
+  const int tid = threadIdx.x;
+  const int c = blockIdx.x;
+  const int P = a.P;
+  const int k1s[2] = {c == 0 ? 0 : c, c == 0 ? P / 2 : P - c};
+  for (int i = tid; i < Q; i += T) roots[i] = __ldg(a.tab.rootsQ + i);
+  float2 G[2][NTR];
+  czt_forward<Q, NTR>(a, c, k1s, buf, roots, gnyq, G);
+  const long long K = a.N / 2 + 1;
+#pragma unroll
+  for (int b = 0; b < 2; ++b) {
+    const long long k = (long long)k1s[b] + (long long)P * tid;
+#pragma unroll
+    for (int t = 0; t < NTR; ++t)
+      if (t < a.Nt) a.F[k + t * K] = G[b][t];
+  }
+  if (c == 0 && tid == 0) {
+    for (int t = 0; t < a.Nt; ++t) a.F[a.N / 2 + t * K] = gnyq[t];
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// Kernel C: inverse four-step pass 2.  grid (Q/TC, pairs).
+// ------------------------------------------------------------------------------------
+template <int P, int TC, int T>
+__global__ void __launch_bounds__(T)
+zdtf_output_kernel(const float2* __restrict__ W, long long N, int Q, int Nr, float* __restrict__ dest,
+                   FusedTables tab) {
+  constexpr int SS = P + 1;
+  extern __shared__ float2 sm[];
+  float2* buf = sm;
+  float2* roots = sm + TC * SS;
+  const int na0 = blockIdx.x * TC;
+  const int q = blockIdx.y;
+  for (int i = threadIdx.x; i < P; i += T) roots[i] = __ldg(tab.rootsP + i);
+  const float2* w = W + (long long)q * P * Q;
+  for (int e = threadIdx.x; e < TC * P; e += T) {
+    const int seq = e % TC, k1 = e / TC;
+    buf[seq * SS + k1] = __ldcs(w + (long long)k1 * Q + na0 + seq);
+  }
+  __syncthreads();
+  smem_fft<P, TC, SS, T, +1>(buf, roots);
+  const int j = 2 * q;
+  float* d0 = dest + (long long)j * N;
+  float* d1 = dest + (long long)(j + 1) * N;
+  const bool has1 = (j + 1) < Nr;
+  for (int e = threadIdx.x; e < TC * P; e += T) {
+    const int seq = e % TC, nb = e / TC;
+    const long long n = (long long)(na0 + seq) + (long long)Q * nb;
+    const float2 v = buf[seq * SS + nb];
+    __stcs(d0 + n, v.x);
+    if (has1) __stcs(d1 + n, v.y);
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// Host side
+// ------------------------------------------------------------------------------------
+// Tile (sequences per CTA) and block size of kernels A and C for a given P.
+template <int P>
+struct AcShape {
+  static constexpr int TILE = P >= 4096 ? 4 : (P >= 2048 ? 8 : 16);
+  static constexpr int T = (TILE * P / 8 > 512) ? 512 : TILE * P / 8;
+  static constexpr size_t SMEM = sizeof(float2) * (TILE * (P + 1) + P);
+};
+
+template <int Q>
+struct CztShape {
+  static constexpr size_t SMEM = sizeof(float2) * (4 * (Q + 1) + 3 * Q + kFusedMaxNt);
+};
+
+bool zdt_fused_eligible(int64_t Nf, int64_t Nt, int64_t Nr) {
+  if (!is_pow2(Nf) || Nt > kFusedMaxNt || Nt < 1 || Nr < 1) return false;
+  const int L = ilog2(Nf);
+  return L >= kFusedMinLog2 && L <= kFusedMaxLog2;
+}
+
+static void float_parts(float x, long long* m, int* e) {
+  if (x == 0.f) { *m = 0; *e = 0; return; }
+  int ex = 0;
+  const float f = frexpf(x, &ex);
+  long long mm = (long long)ldexpf(f, 24);
+  int ee = ex - 24;
+  while (mm != 0 && (mm % 2) == 0) { mm /= 2; ++ee; }
+  *m = mm;
+  *e = ee;
+}
+
+static bool make_phase(float r0, float dr, int L, PhaseInt* ph) {
+  if (!isfinite(r0) || !isfinite(dr)) return false;
+  long long m0, md;
+  int e0, ed;
+  float_parts(r0, &m0, &e0);
+  float_parts(dr, &md, &ed);
+  int s = 0;
+  if (m0 != 0 && -e0 > s) s = -e0;
+  if (md != 0 && -ed > s) s = -ed;
+  const int bits = L + s;
+  if (bits > 62) return false;
+  const unsigned long long mask = (1ULL << bits) - 1ULL;
+  auto part = [&](long long m, int e) -> unsigned long long {
+    if (m == 0) return 0ULL;
+    const int sh = e + s;  // >= 0
+    if (sh >= bits) return 0ULL;
+    return (((unsigned long long)m) << sh) & mask;  // two's complement wrap is exact mod 2^bits
+  };
+  ph->R0 = part(m0, e0);
+  ph->Rd = part(md, ed);
+  ph->mask = mask;
+  ph->bits = bits;
+  ph->scale = ldexpf(1.0f, 1 - bits);
+  return true;
+}
+
+struct FusedState {
+  int L, B;
+  float2* tables = nullptr;  // rootsP | rootsQ | tw_lo | tw_hi
+  FusedTables tab;
+  int64_t NP = 0, npairs = 0;
+};
+
+static std::vector<float2> roots_table(long long n, long long N, long long count) {
+  // exp(-2 pi i m n / N) for m < count, angle reduced exactly in integers
+  std::vector<float2> h((size_t)count);
+  for (long long m = 0; m < count; ++m) {
+    const long long r = (m * n) % N;
+    const double a = -2.0 * (double)r / (double)N;  // half-turns in (-2, 0]
+    h[(size_t)m] = make_float2((float)cos(M_PI * a), (float)sin(M_PI * a));
+  }
+  return h;
+}
+
+#define FDR_FOR_P(X) X(64) X(128) X(256) X(512) X(1024) X(2048) X(4096)
+#define FDR_FOR_Q(X) X(64) X(128) X(256) X(512) X(1024)
+
+static int set_smem_attrs() {
+  static bool done[64] = {false};
+  int dev = 0;
+  FDR_CUDA(cudaGetDevice(&dev));
+  if (dev < 64 && done[dev]) return FDR_OK;
+#define SET_AC(P)                                                                              \
+  FDR_CUDA(cudaFuncSetAttribute(zdtf_input_kernel<P, AcShape<P>::TILE, AcShape<P>::T>,         \
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)AcShape<P>::SMEM)); \
+  FDR_CUDA(cudaFuncSetAttribute(zdtf_output_kernel<P, AcShape<P>::TILE, AcShape<P>::T>,        \
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)AcShape<P>::SMEM));
+  FDR_FOR_P(SET_AC)
+#undef SET_AC
+#define SET_B(Q)                                                                               \
+  FDR_CUDA(cudaFuncSetAttribute(zdtf_czt_kernel<Q, kFusedMaxNt>,                               \
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CztShape<Q>::SMEM)); \
+  FDR_CUDA(cudaFuncSetAttribute(zdtf_a2f_kernel<Q, kFusedMaxNt>,                               \
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CztShape<Q>::SMEM));
+  FDR_FOR_Q(SET_B)
+#undef SET_B
+  if (dev < 64) done[dev] = true;
+  return FDR_OK;
+}
+
+static FusedState* st_of(fdr_zdt* ws) { return reinterpret_cast<FusedState*>(ws->fstate); }
+
+int zdt_fused_setup(fdr_zdt* ws) {
+  const int L = ilog2(ws->Nf);
+  const int Qlog = std::min(10, (L + 1) / 2);
+  ws->fQ = 1 << Qlog;
+  ws->fP = (int)(ws->Nf >> Qlog);
+  FusedState* st = new FusedState();
+  st->L = L;
+  st->B = (L + 1) / 2;
+  st->NP = cdiv(ws->Nt, 2);
+  st->npairs = cdiv(ws->Nr, 2);
+  ws->fstate = st;
+  const long long N = ws->Nf, P = ws->fP, Q = ws->fQ;
+  const long long nlo = 1LL << st->B, nhi = N >> st->B;
+  const long long ntab = P + Q + nlo + nhi;
+  FDR_TRY(set_smem_attrs());
+  cudaError_t e;
+  if ((e = cudaMalloc(&st->tables, sizeof(float2) * ntab)) != cudaSuccess) return cuda_status(e, "cudaMalloc(fused tables)");
+  std::vector<float2> h;
+  auto append = [&](const std::vector<float2>& v) { h.insert(h.end(), v.begin(), v.end()); };
+  append(roots_table(1, P, P));
+  append(roots_table(1, Q, Q));
+  append(roots_table(1, N, nlo));
+  append(roots_table(nlo, N, nhi));
+  if ((e = cudaMemcpy(st->tables, h.data(), sizeof(float2) * ntab, cudaMemcpyHostToDevice)) != cudaSuccess)
+    return cuda_status(e, "upload fused tables");
+  st->tab.rootsP = st->tables;
+  st->tab.rootsQ = st->tables + P;
+  st->tab.tw_lo = st->tables + P + Q;
+  st->tab.tw_hi = st->tables + P + Q + nlo;
+  st->tab.B = st->B;
+  if ((e = cudaMalloc(&ws->A, sizeof(float2) * N * st->NP)) != cudaSuccess) return cuda_status(e, "cudaMalloc(A)");
+  ws->W_pairs = st->npairs;
+  if ((e = cudaMalloc(&ws->W, sizeof(float2) * N * ws->W_pairs)) != cudaSuccess) return cuda_status(e, "cudaMalloc(W)");
+  ws->bytes += (int64_t)sizeof(float2) * (ntab + N * st->NP + N * ws->W_pairs);
+  ws->fused = true;
+  return FDR_OK;
+}
+
+void zdt_fused_release(fdr_zdt* ws) {
+  FusedState* st = st_of(ws);
+  if (st) {
+    cudaFree(st->tables);
+    delete st;
+    ws->fstate = nullptr;
+  }
+  cudaFree(ws->A);
+  cudaFree(ws->W);
+  ws->A = ws->W = nullptr;
+}
+
+int zdt_fused_input(fdr_zdt* ws, const float* spec, cudaStream_t s) {
+  FusedState* st = st_of(ws);
+  const int P = ws->fP, Q = ws->fQ;
+#define LAUNCH_A(PP)                                                                           \
+  if (P == PP) {                                                                               \
+    constexpr int TA = AcShape<PP>::TILE, T = AcShape<PP>::T;                                  \
+    zdtf_input_kernel<PP, TA, T><<<dim3(Q / TA, (unsigned)st->NP), T, AcShape<PP>::SMEM, s>>>( \
+        spec, ws->Nf, (int)ws->Nt, Q, ws->A, st->tab);                                         \
+    FDR_LAUNCH_CHECK("zdtf_input_kernel");                                                     \
+    return FDR_OK;                                                                             \
+  }
+  FDR_FOR_P(LAUNCH_A)
+#undef LAUNCH_A
+  set_error(FDR_ERR_UNSUPPORTED_SIZE, "fused input: P=%d", P);
+  return FDR_ERR_UNSUPPORTED_SIZE;
+}
+
+static CztArgs czt_args(fdr_zdt* ws, FusedState* st) {
+  CztArgs a;
+  memset(&a, 0, sizeof(a));
+  a.A = ws->A;
+  a.W = ws->W;
+  a.N = ws->Nf;
+  a.P = ws->fP;
+  a.Nt = (int)ws->Nt;
+  a.NP = (int)st->NP;
+  a.Nr = (int)ws->Nr;
+  a.npairs = (int)st->npairs;
+  a.tab = st->tab;
+  return a;
+}
+
+int zdt_fused_A_to_F(fdr_zdt* ws, cudaStream_t s) {
+  FusedState* st = st_of(ws);
+  CztArgs a = czt_args(ws, st);
+  a.F = ws->F;
+  const int Q = ws->fQ;
+#define LAUNCH_A2F(QQ)                                                                         \
+  if (Q == QQ) {                                                                               \
+    zdtf_a2f_kernel<QQ, kFusedMaxNt><<<ws->fP / 2, QQ / 2, CztShape<QQ>::SMEM, s>>>(a);        \
+    FDR_LAUNCH_CHECK("zdtf_a2f_kernel");                                                       \
+    return FDR_OK;                                                                             \
+  }
+  FDR_FOR_Q(LAUNCH_A2F)
+#undef LAUNCH_A2F
+  set_error(FDR_ERR_UNSUPPORTED_SIZE, "fused A->F: Q=%d", Q);
+  return FDR_ERR_UNSUPPORTED_SIZE;
+}
+
+int zdt_staged_run(fdr_zdt* ws, float r0, float* dest, int window, const double* wk, cudaStream_t s);
+
+int zdt_fused_run(fdr_zdt* ws, float r0, float* dest, int window, const double* wk,
+                  cudaStream_t s) {
+  FusedState* st = st_of(ws);
+  PhaseInt ph;
+  if (!ws->A_valid || !make_phase(r0, ws->dr, st->L, &ph)) {
+    // No fused input stage to start from (F was set by other means) or rates whose exact
+    // phase does not fit 62 bits: run the staged stages.
+    return zdt_staged_run(ws, r0, dest, window, wk, s);
+  }
+  CztArgs a = czt_args(ws, st);
+  a.ph = ph;
+  a.window = window;
+  a.wk = wk;
+  const int P = ws->fP, Q = ws->fQ;
+  // rate groups: enough CTAs for about four waves of one CTA per SM
+  const int ctas = P / 2;
+  int groups = std::max(1, std::min<int>((int)cdiv(4 * sm_count(), ctas),
+                                         (int)cdiv(st->npairs, kRatesPerBlock / 2)));
+  int ppg = (int)cdiv(st->npairs, groups);
+  ppg = (int)cdiv(ppg, kRatesPerBlock / 2) * (kRatesPerBlock / 2);
+  groups = (int)cdiv(st->npairs, ppg);
+  a.pairs_per_group = ppg;
+  bool launched = false;
+#define LAUNCH_B(QQ)                                                                           \
+  if (Q == QQ) {                                                                               \
+    zdtf_czt_kernel<QQ, kFusedMaxNt><<<dim3(ctas, groups), QQ / 2, CztShape<QQ>::SMEM, s>>>(a); \
+    FDR_LAUNCH_CHECK("zdtf_czt_kernel");                                                       \
+    launched = true;                                                                           \
+  }
+  FDR_FOR_Q(LAUNCH_B)
+#undef LAUNCH_B
+  if (!launched) {
+    set_error(FDR_ERR_UNSUPPORTED_SIZE, "fused czt: Q=%d", Q);
+    return FDR_ERR_UNSUPPORTED_SIZE;
+  }
+  zdt_mark(ws, "czt", s);
+#define LAUNCH_C(PP)                                                                           \
+  if (P == PP) {                                                                               \
+    constexpr int TC = AcShape<PP>::TILE, T = AcShape<PP>::T;                                  \
+    zdtf_output_kernel<PP, TC, T><<<dim3(Q / TC, (unsigned)st->npairs), T, AcShape<PP>::SMEM, s>>>( \
+        ws->W, ws->Nf, Q, (int)ws->Nr, dest, st->tab);                                         \
+    FDR_LAUNCH_CHECK("zdtf_output_kernel");                                                    \
+    zdt_mark(ws, "output", s);                                                                 \
+    return FDR_OK;                                                                             \
+  }
+  FDR_FOR_P(LAUNCH_C)
+#undef LAUNCH_C
+  set_error(FDR_ERR_UNSUPPORTED_SIZE, "fused output: P=%d", P);
+  return FDR_ERR_UNSUPPORTED_SIZE;
+}
 
 }  // namespace fdr

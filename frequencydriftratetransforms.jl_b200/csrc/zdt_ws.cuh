@@ -23,6 +23,7 @@ struct fdr_zdt {
   float2* A = nullptr;           // input-stage intermediate, (Nt/2 rounded up) x fP x fQ
   float2* W = nullptr;           // inverse-stage intermediate for one chunk of rate pairs
   int64_t W_pairs = 0;           // rate pairs held by W
+  void* fstate = nullptr;        // fused-path tables and sizes (zdt_fused.cu)
   bool A_valid = false;          // A holds the spectrogram last given to input!
   bool F_valid = false;          // F holds rfft of that spectrogram
 

@@ -27,8 +27,10 @@ def test_fftfdr_vs_oracle(fdr, oracle, Nf, Nt):
     mws = oracle.fftfdr_workspace(spec)
     assert oracle.rel_linf(out, oracle.fftfdr(mws, rates)) < 2e-5
     assert oracle.rel_linf(out, oracle.fdr_truth(spec, rates)) < 1e-4
+    # a lone column is transformed with a zero partner, a column of fftfdr with its
+    # neighbour (two-for-one real FFT): equal up to float32 rounding
     col = fdr.fdshiftsum(ws, rates[1]).cpu().numpy()
-    np.testing.assert_array_equal(col, out[:, 1])
+    assert oracle.rel_linf(col, out[:, 1]) < 1e-6
 
 
 def test_fdshift_vs_oracle(fdr, oracle):

@@ -1,0 +1,94 @@
+"""GPU parity tests of the fused ZDT kernels (power-of-two Nf, Nt <= 16) against the staged
+kernels and the CPU oracle.
+
+Tolerances (relative L-infinity): 1e-4 vs FP64 (the fused path reduces
+chirp phases exactly and is typically ~1e-6); 2e-5 vs the staged kernels and the FP32
+mirror, which carry the reference's Float32 phase-argument rounding (~5e-6 at Nf=2^20).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _spec(oracle, Nf, Nt, seed, ntones=3):
+    spec, _ = oracle.synth_spectrogram(Nf, Nt, ntones, 20.0, 20.0, 4.0, seed=seed)
+    return spec
+
+
+@pytest.mark.parametrize("Nf,Nt,r0,dr,Nr", [
+    (4096, 16, -4.0, 0.25, 33), (4096, 7, 1.5, -0.125, 8), (8192, 16, -2.0, 1 / 16, 5),
+    (2 ** 13, 2, 0.0, 0.5, 1), (2 ** 15, 15, -3.0, 0.1, 2), (2 ** 17, 16, -4.0, 0.25, 33),
+    (2 ** 21, 4, -1.0, 0.25, 9), (2 ** 22, 2, 0.5, 1.0, 3)])
+def test_fused_vs_truth_and_staged(fdr, oracle, Nf, Nt, r0, dr, Nr):
+    spec = _spec(oracle, Nf, Nt, seed=Nf + Nt)
+    ws = fdr.ZDTWorkspace(spec, r0, dr, Nr)
+    assert ws.fused
+    out = fdr.zdtfdr(ws).cpu().numpy()
+    rates = [float(np.float32(r0)) + j * float(np.float32(dr)) for j in range(Nr)]
+    cols = list(range(Nr)) if Nf <= 2 ** 17 else [0, Nr - 1]
+    truth = oracle.fdr_truth(spec, [rates[j] for j in cols])
+    err = oracle.rel_linf(out[:, cols], truth)
+    assert err < 1e-5, err
+    st = fdr.ZDTWorkspace(spec, r0, dr, Nr, staged_only=True)
+    assert not st.fused
+    assert oracle.rel_linf(out, fdr.zdtfdr(st).cpu().numpy()) < 2e-5
+
+
+def test_config2_fused(fdr, oracle):
+    """Nf=2^20, Nt=16, rates -4:1/16:4 (129) -- the benchmark workload."""
+    spec, _ = oracle.synth_spectrogram(2 ** 20, 16, 20, 8.0, 50.0, 4.0, seed=2000)
+    ws = fdr.ZDTWorkspace(spec, -4.0, 1 / 16, 129)
+    assert ws.fused and ws.Nl == 144
+    out = fdr.zdtfdr(ws).cpu().numpy()
+    cols = [0, 3, 37, 64, 100, 128]
+    truth = oracle.fdr_truth(spec, [-4.0 + j / 16 for j in cols])
+    err = oracle.rel_linf(out[:, cols], truth)
+    assert err < 1e-5, err
+    # integer drift rates are exact circular-shift sums
+    icols = [0, 16, 32, 48, 64, 80, 96, 112, 128]
+    ref = oracle.intfdr(spec, [-4 + j // 16 for j in icols])
+    assert oracle.rel_linf(out[:, icols], ref) < 1e-5
+    # and the reference's FP32 stage sequence agrees within its own phase rounding
+    staged = fdr.zdtfdr(fdr.ZDTWorkspace(spec, -4.0, 1 / 16, 129, staged_only=True)).cpu().numpy()
+    assert oracle.rel_linf(out, staged) < 2e-5
+
+
+def test_fused_windows_and_batches(fdr, oracle):
+    spec = _spec(oracle, 2 ** 14, 16, seed=5)
+    ws = fdr.ZDTWorkspace(spec, -2.0, 0.25, 17)
+    st = fdr.ZDTWorkspace(spec, -2.0, 0.25, 17, staged_only=True)
+    for w in ("hamming", lambda n, N: 1.0 - n / N):
+        a = fdr.zdtfdr(ws, w=w).cpu().numpy()
+        b = fdr.zdtfdr(st, w=w).cpu().numpy()
+        assert oracle.rel_linf(a, b) < 2e-5
+    dests = [fdr.fortran_empty(2 ** 14, 17) for _ in range(3)]
+    fdr.zdtfdr_(dests, ws, r0=[-6.0, -1.75, 2.5])
+    for d, r0 in zip(dests, [-6.0, -1.75, 2.5]):
+        truth = oracle.fdr_truth(spec, [r0 + 0.25 * j for j in range(17)])
+        assert oracle.rel_linf(d.cpu().numpy(), truth) < 1e-5
+
+
+def test_fused_input_then_staged_stages(fdr, oracle):
+    """input! through the fused path, then the staged stages read F (rebuilt from the fused
+    input stage) -- equal to a staged-only workspace's F."""
+    spec = _spec(oracle, 2 ** 15, 16, seed=9)
+    ws = fdr.ZDTWorkspace(spec, -1.0, 0.5, 5)
+    st = fdr.ZDTWorkspace(spec, -1.0, 0.5, 5, staged_only=True)
+    F1, F2 = ws.F.cpu().numpy(), st.F.cpu().numpy()
+    assert np.abs(F1 - F2).max() / np.abs(F2).max() < 1e-6
+    fdr.zdtfdr_nodest_(ws)
+    d = fdr.fortran_empty(2 ** 15, 5)
+    fdr.output_(d, ws)
+    truth = oracle.fdr_truth(spec, [-1.0 + 0.5 * j for j in range(5)])
+    assert oracle.rel_linf(d.cpu().numpy(), truth) < 1e-5
+
+
+def test_fused_phase_fallback(fdr, oracle):
+    """A rate step whose exact phase needs more than 62 bits runs the staged kernels."""
+    spec = _spec(oracle, 4096, 8, seed=13)
+    dr = 2.0 ** -60
+    ws = fdr.ZDTWorkspace(spec, 1.0, dr, 3)
+    out = fdr.zdtfdr(ws).cpu().numpy()
+    truth = oracle.fdr_truth(spec, [1.0, 1.0 + dr, 1.0 + 2 * dr])
+    assert oracle.rel_linf(out, truth) < 1e-5
