@@ -157,6 +157,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--staged", action="store_true", help="force the staged ZDT kernels")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -226,9 +227,9 @@ def main():
     # ---------------- end-to-end through the public API (host buffers) ----------------
     pinned = [torch.from_numpy(h.T.copy()).pin_memory() for h in host_specs]  # (Nt, Nf) rows
     dev_in = fdr.fortran_empty(NF, NT)
-    e2e_steps = max(3, min(args.steps, 10))
+    e2e_steps = 0 if args.no_e2e else max(3, min(args.steps, 10))
     nh_total = 0
-    for i in range(2):
+    for i in range(2 if e2e_steps else 0):
         dev_in.t().copy_(pinned[i % nbuf], non_blocking=True)
         fdr.zdtfdr_(dest, ws, dev_in)
         fdr.findprotohits(dest, HIT_SNR, snr=True)
@@ -246,7 +247,7 @@ def main():
         t = torch.tensor([e2e_s], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    e2e_value = NF * NR * e2e_steps * world / e2e_s
+    e2e_value = NF * NR * e2e_steps * world / e2e_s if e2e_steps else None
 
     # ---------------- roofline of the ZDT call ----------------
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -279,7 +280,7 @@ def main():
                              "FDR output per step"},
             "e2e": {"value": e2e_value, "unit": "cells/s",
                     "h2d_bytes_per_step": 4 * NF * NT,
-                    "d2h_bytes_per_step": int(16 * nh_total / e2e_steps) + 8,
+                    "d2h_bytes_per_step": int(16 * nh_total / max(1, e2e_steps)) + 8,
                     "path": "pinned host spectrogram -> zdtfdr! -> findprotohits(snr=10) -> host"},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -58,6 +58,44 @@ struct Dft<8> {
 };
 
 template <>
+struct Dft<16> {
+  // 4 x 4 decomposition: r = r1 + 4*r2, m = m2 + 4*m1
+  __device__ __forceinline__ static void run(float2* v, int sign) {
+    // cos / sin of 2*pi*e/16, e = 0..9
+    const float C[10] = {1.f, 0.92387953251128675613f, 0.70710678118654752440f,
+                         0.38268343236508977173f, 0.f, -0.38268343236508977173f,
+                         -0.70710678118654752440f, -0.92387953251128675613f, -1.f,
+                         -0.92387953251128675613f};
+    const float S[10] = {0.f, 0.38268343236508977173f, 0.70710678118654752440f,
+                         0.92387953251128675613f, 1.f, 0.92387953251128675613f,
+                         0.70710678118654752440f, 0.38268343236508977173f, 0.f,
+                         -0.38268343236508977173f};
+    float2 y[4][4];
+#pragma unroll
+    for (int r1 = 0; r1 < 4; ++r1) {
+      float2 t[4] = {v[r1], v[r1 + 4], v[r1 + 8], v[r1 + 12]};
+      Dft<4>::run(t, sign);
+#pragma unroll
+      for (int m2 = 0; m2 < 4; ++m2) y[r1][m2] = t[m2];
+    }
+#pragma unroll
+    for (int r1 = 1; r1 < 4; ++r1)
+#pragma unroll
+      for (int m2 = 1; m2 < 4; ++m2) {
+        const int e = r1 * m2;
+        y[r1][m2] = cmul(y[r1][m2], make_float2(C[e], sign * S[e]));
+      }
+#pragma unroll
+    for (int m2 = 0; m2 < 4; ++m2) {
+      float2 t[4] = {y[0][m2], y[1][m2], y[2][m2], y[3][m2]};
+      Dft<4>::run(t, sign);
+#pragma unroll
+      for (int m1 = 0; m1 < 4; ++m1) v[m2 + 4 * m1] = t[m1];
+    }
+  }
+};
+
+template <>
 struct Dft<3> {
   __device__ __forceinline__ static void run(float2* v, int sign) {
     const float c = -0.5f, sn = 0.86602540378443864676f;
@@ -91,10 +129,16 @@ struct Dft<5> {
   }
 };
 
+// Shared-memory layout of an FFT sequence: element i is stored at pidx(i) = i + i/8 within
+// a sequence of padded stride padlen(LEN); the pad breaks the bank conflicts of the
+// power-of-two strides of the Stockham passes.
+__host__ __device__ constexpr int padlen(int len) { return len + len / 8; }
+__device__ __forceinline__ int pidx(int i) { return i + (i >> 3); }
+
 // One radix-R Stockham pass over NSEQ power-of-two sequences of length LEN stored at
-// buf[seq*SSTRIDE + i], in place: every thread first reads the inputs of its butterflies
-// into registers, the block synchronises, then the outputs are written.  roots[m] =
-// exp(-2*pi*i*m/LEN) (shared or global memory).
+// buf[seq*SSTRIDE + pidx(i)], in place: every thread first reads the inputs of its
+// butterflies into registers, the block synchronises, then the outputs are written.
+// roots[m] = exp(-2*pi*i*m/LEN) (shared or global memory).
 template <int LEN, int NSEQ, int SSTRIDE, int T, int SIGN, int NS, int R>
 __device__ __forceinline__ void stockham_pass(float2* buf, const float2* roots) {
   constexpr int NBF = LEN / R;             // butterflies per sequence
@@ -107,9 +151,9 @@ __device__ __forceinline__ void stockham_pass(float2* buf, const float2* roots) 
     const int j = threadIdx.x + i * T;
     if (NB % T == 0 || j < NB) {
       const int seq = j / NBF, jj = j - seq * NBF;
-      const float2* a = buf + seq * SSTRIDE + jj;
+      const float2* a = buf + seq * SSTRIDE;
 #pragma unroll
-      for (int r = 0; r < R; ++r) v[i][r] = a[r * NBF];
+      for (int r = 0; r < R; ++r) v[i][r] = a[pidx(jj + r * NBF)];
     }
   }
   __syncthreads();
@@ -128,9 +172,10 @@ __device__ __forceinline__ void stockham_pass(float2* buf, const float2* roots) 
         }
       }
       Dft<R>::run(v[i], SIGN);
-      float2* b = buf + seq * SSTRIDE + (jj / NS) * NS * R + k;
+      float2* b = buf + seq * SSTRIDE;
+      const int base = (jj / NS) * NS * R + k;
 #pragma unroll
-      for (int r = 0; r < R; ++r) b[r * NS] = v[i][r];
+      for (int r = 0; r < R; ++r) b[pidx(base + r * NS)] = v[i][r];
     }
   }
   __syncthreads();
@@ -140,18 +185,21 @@ template <int LEN, int NSEQ, int SSTRIDE, int T, int SIGN, int NS>
 __device__ __forceinline__ void stockham_passes(float2* buf, const float2* roots) {
   if constexpr (NS < LEN) {
     constexpr int REM = LEN / NS;
-    constexpr int R = (REM % 8 == 0) ? 8 : ((REM % 4 == 0) ? 4 : 2);
+    constexpr int R = (REM % 16 == 0 && REM != 32) ? 16
+                      : ((REM % 8 == 0) ? 8 : ((REM % 4 == 0) ? 4 : 2));
     stockham_pass<LEN, NSEQ, SSTRIDE, T, SIGN, NS, R>(buf, roots);
     stockham_passes<LEN, NSEQ, SSTRIDE, T, SIGN, NS * R>(buf, roots);
   }
 }
 
 // In-place FFT (natural order in and out) of NSEQ sequences of power-of-two length LEN
-// held at buf[seq*SSTRIDE + i].  Must be called by all T threads of the block; the caller
-// synchronises before (the inputs are visible) and may rely on a barrier at the end.
+// held at buf[seq*SSTRIDE + pidx(i)] (SSTRIDE >= padlen(LEN)).  Must be called by all T
+// threads of the block; the caller synchronises before (the inputs are visible); the
+// function ends with a barrier.
 template <int LEN, int NSEQ, int SSTRIDE, int T, int SIGN>
 __device__ __forceinline__ void smem_fft(float2* buf, const float2* roots) {
   static_assert((LEN & (LEN - 1)) == 0, "power-of-two length");
+  static_assert(SSTRIDE >= padlen(LEN), "sequence stride too small");
   stockham_passes<LEN, NSEQ, SSTRIDE, T, SIGN, 1>(buf, roots);
 }
 

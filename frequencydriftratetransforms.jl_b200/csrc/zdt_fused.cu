@@ -37,7 +37,15 @@ namespace fdr {
 constexpr int kFusedMinLog2 = 12;
 constexpr int kFusedMaxLog2 = 22;
 constexpr int kFusedMaxNt = 16;
-constexpr int kRatesPerBlock = 4;  // 2 rate pairs per inverse-FFT block in kernel B
+constexpr int kRatesPerBlock = 8;  // 4 rate pairs (8 sequences) per inverse-FFT block in kernel B
+constexpr int kHorner = 4;         // rates evaluated together by one thread (a half block)
+
+// Shared-memory stride of one FFT sequence of kernels A and C (TILE sequences per CTA):
+// padded length plus an offset that spreads the TILE sequences over distinct banks.
+template <int P, int TILE>
+__host__ __device__ constexpr int ac_stride() { return padlen(P) + 16 / TILE; }
+template <int Q>
+__host__ __device__ constexpr int b_stride() { return padlen(Q) + 1; }
 
 struct PhaseInt {
   unsigned long long R0, Rd, mask;
@@ -72,7 +80,7 @@ template <int P, int TA, int T>
 __global__ void __launch_bounds__(T)
 zdtf_input_kernel(const float* __restrict__ spec, long long N, int Nt, int Q,
                   float2* __restrict__ A, FusedTables tab) {
-  constexpr int SS = P + 1;
+  constexpr int SS = ac_stride<P, TA>();
   extern __shared__ float2 sm[];
   float2* buf = sm;
   float2* roots = sm + TA * SS;
@@ -87,7 +95,7 @@ zdtf_input_kernel(const float* __restrict__ spec, long long N, int Nt, int Q,
     const long long n = (long long)(na0 + seq) + (long long)Q * nb;
     const float a = __ldcs(c0 + n);
     const float b = has1 ? __ldcs(c1 + n) : 0.f;
-    buf[seq * SS + nb] = make_float2(a, b);
+    buf[seq * SS + pidx(nb)] = make_float2(a, b);
   }
   __syncthreads();
   smem_fft<P, TA, SS, T, -1>(buf, roots);
@@ -95,7 +103,7 @@ zdtf_input_kernel(const float* __restrict__ spec, long long N, int Nt, int Q,
     const int seq = e % TA, k1 = e / TA;
     const int na = na0 + seq;
     const float2 w = tw_fwd(tab, (long long)k1 * na);
-    A[((long long)p * P + k1) * Q + na] = cmul(buf[seq * SS + k1], w);
+    A[((long long)p * P + k1) * Q + na] = cmul(buf[seq * SS + pidx(k1)], w);
   }
 }
 
@@ -122,50 +130,58 @@ __device__ __forceinline__ void mirror_of(int c, int side, int k2, int Q, int* m
 
 // Forward pass 2 + two-for-one unpack: G[b][t] = F[k_b, t] for the two bases of this
 // thread (b = side, k2 = threadIdx.x); CTA 0's thread 0 also stores the Nyquist bin's
-// F[N/2, t] into gnyq (shared memory).  buf holds 4 sequences of stride Q+1.
+// F[N/2, t] into gnyq (shared memory).  buf holds 8 sequences of stride b_stride<Q>().
 template <int Q, int NTR>
 __device__ __forceinline__ void czt_forward(const CztArgs& a, int c, const int* k1s, float2* buf,
                                             const float2* roots, float2* gnyq,
                                             float2 (&G)[2][NTR]) {
   constexpr int T = Q / 2;
-  constexpr int SS = Q + 1;
+  constexpr int SS = b_stride<Q>();
+  constexpr int PC = 4;  // t pairs per chunk (8 sequences: 4 pairs x 2 sides)
   const int tid = threadIdx.x;
 #pragma unroll
   for (int b = 0; b < 2; ++b)
 #pragma unroll
     for (int t = 0; t < NTR; ++t) G[b][t] = make_float2(0.f, 0.f);
+  // Only thread 0 of CTA 0 touches gnyq; t-pairs beyond Nt are never loaded, so clear all.
+  if (c == 0 && tid == 0)
+    for (int t = 0; t < NTR; ++t) gnyq[t] = make_float2(0.f, 0.f);
 #pragma unroll
-  for (int p0 = 0; p0 < NTR / 2; p0 += 2) {
+  for (int p0 = 0; p0 < NTR / 2; p0 += PC) {
     if (p0 < a.NP) {
       __syncthreads();
-      for (int e = tid; e < 4 * Q; e += T) {
+      for (int e = tid; e < 2 * PC * Q; e += T) {
         const int seq = e / Q, na = e - seq * Q;
         const int pp = p0 + (seq >> 1), side = seq & 1;
         float2 v = make_float2(0.f, 0.f);
         if (pp < a.NP) v = a.A[((long long)pp * a.P + k1s[side]) * Q + na];
-        buf[seq * SS + na] = v;
+        buf[seq * SS + pidx(na)] = v;
       }
       __syncthreads();
-      smem_fft<Q, 4, SS, T, -1>(buf, roots);
+      smem_fft<Q, 2 * PC, SS, T, -1>(buf, roots);
 #pragma unroll
       for (int b = 0; b < 2; ++b) {
         int ms, mk2;
         mirror_of(c, b, tid, Q, &ms, &mk2);
 #pragma unroll
-        for (int u = 0; u < 2; ++u) {
-          const float2 zk = buf[(2 * u + b) * SS + tid];
-          const float2 zm = cconj(buf[(2 * u + ms) * SS + mk2]);
-          const float2 s = cadd(zk, zm), d = csub(zk, zm);
-          G[b][2 * (p0 + u)] = make_float2(0.5f * s.x, 0.5f * s.y);
-          G[b][2 * (p0 + u) + 1] = make_float2(0.5f * d.y, -0.5f * d.x);
+        for (int u = 0; u < PC; ++u) {
+          if (2 * (p0 + u) + 1 < NTR) {
+            const float2 zk = buf[(2 * u + b) * SS + pidx(tid)];
+            const float2 zm = cconj(buf[(2 * u + ms) * SS + pidx(mk2)]);
+            const float2 sm_ = cadd(zk, zm), d = csub(zk, zm);
+            G[b][2 * (p0 + u)] = make_float2(0.5f * sm_.x, 0.5f * sm_.y);
+            G[b][2 * (p0 + u) + 1] = make_float2(0.5f * d.y, -0.5f * d.x);
+          }
         }
       }
       if (c == 0 && tid == 0) {
 #pragma unroll
-        for (int u = 0; u < 2; ++u) {
-          const float2 z = buf[(2 * u) * SS + Q / 2];
-          gnyq[2 * (p0 + u)] = make_float2(z.x, 0.f);
-          gnyq[2 * (p0 + u) + 1] = make_float2(z.y, 0.f);
+        for (int u = 0; u < PC; ++u) {
+          if (2 * (p0 + u) + 1 < NTR) {
+            const float2 z = buf[(2 * u) * SS + pidx(Q / 2)];
+            gnyq[2 * (p0 + u)] = make_float2(z.x, 0.f);
+            gnyq[2 * (p0 + u) + 1] = make_float2(z.y, 0.f);
+          }
         }
       }
     }
@@ -195,10 +211,10 @@ __device__ __forceinline__ float window_value(const CztArgs& a, long long k) {
 template <int Q, int NTR>
 __global__ void __launch_bounds__(Q / 2, 1) zdtf_czt_kernel(CztArgs a) {
   constexpr int T = Q / 2;
-  constexpr int SS = Q + 1;
+  constexpr int SS = b_stride<Q>();
   extern __shared__ float2 sm[];
-  float2* buf = sm;                // 4 * SS
-  float2* roots = buf + 4 * SS;    // Q
+  float2* buf = sm;                // kRatesPerBlock * SS
+  float2* roots = buf + kRatesPerBlock * SS;  // Q
   float2* twr = roots + Q;         // 2 * Q
   float2* gnyq = twr + 2 * Q;      // NTR
   const int tid = threadIdx.x;
@@ -214,10 +230,11 @@ __global__ void __launch_bounds__(Q / 2, 1) zdtf_czt_kernel(CztArgs a) {
   float2 G[2][NTR];
   czt_forward<Q, NTR>(a, c, k1s, buf, roots, gnyq, G);
 
-  // Per-base phase state: w_{k,j} = exp(2 pi i (alpha + j*beta) / 2^bits)
+  // Per-base phase state: w_{k,j} = exp(2 pi i (alpha + j*beta) / 2^bits); rates are taken
+  // kHorner at a time, w = w(first rate of the group, exact) * pw[jr] (exact).
   const unsigned long long mask = a.ph.mask;
   unsigned long long alpha[2], beta[2];
-  float2 pw[2][kRatesPerBlock];
+  float2 pw[2][kHorner];
   float win[2];
 #pragma unroll
   for (int b = 0; b < 2; ++b) {
@@ -225,7 +242,7 @@ __global__ void __launch_bounds__(Q / 2, 1) zdtf_czt_kernel(CztArgs a) {
     alpha[b] = (k * a.ph.R0) & mask;
     beta[b] = (k * a.ph.Rd) & mask;
 #pragma unroll
-    for (int i = 0; i < kRatesPerBlock; ++i) pw[b][i] = cis_phase(((unsigned long long)i * beta[b]) & mask, a.ph);
+    for (int i = 0; i < kHorner; ++i) pw[b][i] = cis_phase(((unsigned long long)i * beta[b]) & mask, a.ph);
     win[b] = window_value(a, (long long)k);
   }
   // Nyquist bin (CTA 0, thread 0)
@@ -241,29 +258,34 @@ __global__ void __launch_bounds__(Q / 2, 1) zdtf_czt_kernel(CztArgs a) {
   const int q_end = min(a.npairs, q_begin + a.pairs_per_group);
   for (int q0 = q_begin; q0 < q_end; q0 += kRatesPerBlock / 2) {
     const int j0 = 2 * q0;
-    float2 S[2][kRatesPerBlock];
-#pragma unroll
-    for (int b = 0; b < 2; ++b) {
-      const float2 w0 = cis_phase((alpha[b] + (unsigned long long)j0 * beta[b]) & mask, a.ph);
-#pragma unroll
-      for (int jr = 0; jr < kRatesPerBlock; ++jr) {
-        const float2 w = cmul(w0, pw[b][jr]);
-        float2 s = horner<NTR>(G[b], w);
-        if (j0 + jr >= a.Nr) s = make_float2(0.f, 0.f);
-        S[b][jr] = cscale(s, win[b]);
-      }
-    }
     __syncthreads();  // buf is free
 #pragma unroll
-    for (int b = 0; b < 2; ++b) {
+    for (int h = 0; h < kRatesPerBlock / kHorner; ++h) {
+      const int jh = j0 + h * kHorner;
+      float2 S[2][kHorner];
 #pragma unroll
-      for (int u = 0; u < kRatesPerBlock / 2; ++u) {
-        const float2 sa = S[b][2 * u], sb = S[b][2 * u + 1];
-        if (dc && b == 0) {
-          buf[(2 * u) * SS + 0] = make_float2(sa.x, sb.x);  // real-only DC bin
-        } else {
-          buf[(2 * u + b) * SS + tid] = make_float2(sa.x - sb.y, sa.y + sb.x);       // sa + i sb
-          buf[(2 * u + ms[b]) * SS + mk2[b]] = make_float2(sa.x + sb.y, sb.x - sa.y);  // conj(sa) + i conj(sb)
+      for (int b = 0; b < 2; ++b) {
+        const float2 w0 = cis_phase((alpha[b] + (unsigned long long)jh * beta[b]) & mask, a.ph);
+#pragma unroll
+        for (int jr = 0; jr < kHorner; ++jr) {
+          const float2 w = cmul(w0, pw[b][jr]);
+          float2 sv = horner<NTR>(G[b], w);
+          if (jh + jr >= a.Nr) sv = make_float2(0.f, 0.f);
+          S[b][jr] = cscale(sv, win[b]);
+        }
+      }
+#pragma unroll
+      for (int b = 0; b < 2; ++b) {
+#pragma unroll
+        for (int u2 = 0; u2 < kHorner / 2; ++u2) {
+          const int u = h * (kHorner / 2) + u2;  // rate pair within the block
+          const float2 sa = S[b][2 * u2], sb = S[b][2 * u2 + 1];
+          if (dc && b == 0) {
+            buf[(2 * u) * SS + pidx(0)] = make_float2(sa.x, sb.x);  // real-only DC bin
+          } else {
+            buf[(2 * u + b) * SS + pidx(tid)] = make_float2(sa.x - sb.y, sa.y + sb.x);          // sa + i sb
+            buf[(2 * u + ms[b]) * SS + pidx(mk2[b])] = make_float2(sa.x + sb.y, sb.x - sa.y);  // conj(sa) + i conj(sb)
+          }
         }
       }
     }
@@ -272,17 +294,16 @@ __global__ void __launch_bounds__(Q / 2, 1) zdtf_czt_kernel(CztArgs a) {
 #pragma unroll
       for (int t = 0; t < NTR; ++t) Gn[t] = gnyq[t];
       const float wn = window_value(a, (long long)kny);
-#pragma unroll
       for (int u = 0; u < kRatesPerBlock / 2; ++u) {
         float v[2];
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const int j = j0 + 2 * u + h;
+        for (int hh = 0; hh < 2; ++hh) {
+          const int j = j0 + 2 * u + hh;
           const float2 w = cis_phase((alpha_n + (unsigned long long)j * beta_n) & mask, a.ph);
-          const float2 s = horner<NTR>(Gn, w);
-          v[h] = (j < a.Nr) ? s.x * wn : 0.f;  // real-only Nyquist bin
+          const float2 sv = horner<NTR>(Gn, w);
+          v[hh] = (j < a.Nr) ? sv.x * wn : 0.f;  // real-only Nyquist bin
         }
-        buf[(2 * u) * SS + Q / 2] = make_float2(v[0], v[1]);
+        buf[(2 * u) * SS + pidx(Q / 2)] = make_float2(v[0], v[1]);
       }
     }
     __syncthreads();
@@ -291,7 +312,7 @@ __global__ void __launch_bounds__(Q / 2, 1) zdtf_czt_kernel(CztArgs a) {
       const int seq = e / Q, na = e - seq * Q;
       const int q = q0 + (seq >> 1), side = seq & 1;
       if (q < q_end)
-        a.W[((long long)q * P + k1s[side]) * Q + na] = cmul(buf[seq * SS + na], twr[side * Q + na]);
+        a.W[((long long)q * P + k1s[side]) * Q + na] = cmul(buf[seq * SS + pidx(na)], twr[side * Q + na]);
     }
   }
 }
@@ -300,10 +321,10 @@ __global__ void __launch_bounds__(Q / 2, 1) zdtf_czt_kernel(CztArgs a) {
 template <int Q, int NTR>
 __global__ void __launch_bounds__(Q / 2, 1) zdtf_a2f_kernel(CztArgs a) {
   constexpr int T = Q / 2;
-  constexpr int SS = Q + 1;
+  constexpr int SS = b_stride<Q>();
   extern __shared__ float2 sm[];
   float2* buf = sm;
-  float2* roots = buf + 4 * SS;
+  float2* roots = buf + kRatesPerBlock * SS;
   float2* twr = roots + Q;
   float2* gnyq = twr + 2 * Q;
   const int tid = threadIdx.x;
@@ -311,6 +332,7 @@ __global__ void __launch_bounds__(Q / 2, 1) zdtf_a2f_kernel(CztArgs a) {
   const int P = a.P;
   const int k1s[2] = {c == 0 ? 0 : c, c == 0 ? P / 2 : P - c};
   for (int i = tid; i < Q; i += T) roots[i] = __ldg(a.tab.rootsQ + i);
+  (void)twr;
   float2 G[2][NTR];
   czt_forward<Q, NTR>(a, c, k1s, buf, roots, gnyq, G);
   const long long K = a.N / 2 + 1;
@@ -333,7 +355,7 @@ template <int P, int TC, int T>
 __global__ void __launch_bounds__(T)
 zdtf_output_kernel(const float2* __restrict__ W, long long N, int Q, int Nr, float* __restrict__ dest,
                    FusedTables tab) {
-  constexpr int SS = P + 1;
+  constexpr int SS = ac_stride<P, TC>();
   extern __shared__ float2 sm[];
   float2* buf = sm;
   float2* roots = sm + TC * SS;
@@ -343,7 +365,7 @@ zdtf_output_kernel(const float2* __restrict__ W, long long N, int Q, int Nr, flo
   const float2* w = W + (long long)q * P * Q;
   for (int e = threadIdx.x; e < TC * P; e += T) {
     const int seq = e % TC, k1 = e / TC;
-    buf[seq * SS + k1] = __ldcs(w + (long long)k1 * Q + na0 + seq);
+    buf[seq * SS + pidx(k1)] = __ldcs(w + (long long)k1 * Q + na0 + seq);
   }
   __syncthreads();
   smem_fft<P, TC, SS, T, +1>(buf, roots);
@@ -354,7 +376,7 @@ zdtf_output_kernel(const float2* __restrict__ W, long long N, int Q, int Nr, flo
   for (int e = threadIdx.x; e < TC * P; e += T) {
     const int seq = e % TC, nb = e / TC;
     const long long n = (long long)(na0 + seq) + (long long)Q * nb;
-    const float2 v = buf[seq * SS + nb];
+    const float2 v = buf[seq * SS + pidx(nb)];
     __stcs(d0 + n, v.x);
     if (has1) __stcs(d1 + n, v.y);
   }
@@ -363,17 +385,18 @@ zdtf_output_kernel(const float2* __restrict__ W, long long N, int Q, int Nr, flo
 // ------------------------------------------------------------------------------------
 // Host side
 // ------------------------------------------------------------------------------------
-// Tile (sequences per CTA) and block size of kernels A and C for a given P.
+// Tile (sequences per CTA) and block size of kernels A and C for a given P: one radix-16
+// butterfly per thread per pass, about 75 KB of shared memory, two CTAs per SM.
 template <int P>
 struct AcShape {
-  static constexpr int TILE = P >= 4096 ? 4 : (P >= 2048 ? 8 : 16);
-  static constexpr int T = (TILE * P / 8 > 512) ? 512 : TILE * P / 8;
-  static constexpr size_t SMEM = sizeof(float2) * (TILE * (P + 1) + P);
+  static constexpr int TILE = P >= 4096 ? 4 : 8;
+  static constexpr int T = (TILE * P / 16 > 512) ? 512 : (TILE * P / 16 < 32 ? 32 : TILE * P / 16);
+  static constexpr size_t SMEM = sizeof(float2) * (TILE * ac_stride<P, TILE>() + P);
 };
 
 template <int Q>
 struct CztShape {
-  static constexpr size_t SMEM = sizeof(float2) * (4 * (Q + 1) + 3 * Q + kFusedMaxNt);
+  static constexpr size_t SMEM = sizeof(float2) * (kRatesPerBlock * b_stride<Q>() + 3 * Q + kFusedMaxNt);
 };
 
 bool zdt_fused_eligible(int64_t Nf, int64_t Nt, int64_t Nr) {
