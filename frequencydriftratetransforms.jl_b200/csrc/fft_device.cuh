@@ -129,22 +129,40 @@ struct Dft<5> {
   }
 };
 
-// Shared-memory layout of an FFT sequence: element i is stored at pidx(i) = i + i/8 within
-// a sequence of padded stride padlen(LEN); the pad breaks the bank conflicts of the
-// power-of-two strides of the Stockham passes.
-__host__ __device__ constexpr int padlen(int len) { return len + len / 8; }
-__device__ __forceinline__ int pidx(int i) { return i + (i >> 3); }
+// Shared-memory layout of an FFT sequence: element i is stored at pidx(i) = i + i/16
+// within a sequence of padded stride padlen(LEN).  With the radix plan below every
+// half-warp of a Stockham pass then reads and writes 16 distinct 8-byte bank pairs.
+__host__ __device__ constexpr int padlen(int len) { return len + len / 16; }
+__device__ __forceinline__ int pidx(int i) { return i + (i >> 4); }
+
+// Radix of the pass that starts with NS (= product of the earlier radices) for length LEN.
+__host__ __device__ constexpr int plan_radix(int rem) {
+  return (rem % 16 == 0 && rem != 32) ? 16 : ((rem % 8 == 0) ? 8 : ((rem % 4 == 0) ? 4 : 2));
+}
+// Offset, in a per-length twiddle table, of the pass that starts at NS.  The table holds,
+// for each pass with NS > 1, exp(-2*pi*i*r*k/(NS*R)) at [(r-1)*NS + k] (r in [1,R), k < NS),
+// so that threads with consecutive k read consecutive entries.
+__host__ __device__ constexpr int tw_offset(int len, int ns_target) {
+  int off = 0, ns = 1;
+  while (ns < ns_target) {
+    const int R = plan_radix(len / ns);
+    if (ns > 1) off += (R - 1) * ns;
+    ns *= R;
+  }
+  return off;
+}
+__host__ __device__ constexpr int tw_size(int len) { return tw_offset(len, len); }
 
 // One radix-R Stockham pass over NSEQ power-of-two sequences of length LEN stored at
 // buf[seq*SSTRIDE + pidx(i)], in place: every thread first reads the inputs of its
 // butterflies into registers, the block synchronises, then the outputs are written.
-// roots[m] = exp(-2*pi*i*m/LEN) (shared or global memory).
+// twt is the per-length twiddle table (tw_offset layout, forward sign).
 template <int LEN, int NSEQ, int SSTRIDE, int T, int SIGN, int NS, int R>
-__device__ __forceinline__ void stockham_pass(float2* buf, const float2* roots) {
+__device__ __forceinline__ void stockham_pass(float2* buf, const float2* twt) {
   constexpr int NBF = LEN / R;             // butterflies per sequence
   constexpr int NB = NBF * NSEQ;           // butterflies in total
   constexpr int PER = (NB + T - 1) / T;    // per thread
-  constexpr int TWS = LEN / (NS * R);      // roots stride
+  const float2* tw = twt + tw_offset(LEN, NS);
   float2 v[PER][R];
 #pragma unroll
   for (int i = 0; i < PER; ++i) {
@@ -166,7 +184,7 @@ __device__ __forceinline__ void stockham_pass(float2* buf, const float2* roots) 
       if (NS > 1) {
 #pragma unroll
         for (int r = 1; r < R; ++r) {
-          float2 w = roots[r * k * TWS];
+          float2 w = tw[(r - 1) * NS + k];
           if (SIGN > 0) w.y = -w.y;
           v[i][r] = cmul(v[i][r], w);
         }
@@ -182,25 +200,24 @@ __device__ __forceinline__ void stockham_pass(float2* buf, const float2* roots) 
 }
 
 template <int LEN, int NSEQ, int SSTRIDE, int T, int SIGN, int NS>
-__device__ __forceinline__ void stockham_passes(float2* buf, const float2* roots) {
+__device__ __forceinline__ void stockham_passes(float2* buf, const float2* twt) {
   if constexpr (NS < LEN) {
-    constexpr int REM = LEN / NS;
-    constexpr int R = (REM % 16 == 0 && REM != 32) ? 16
-                      : ((REM % 8 == 0) ? 8 : ((REM % 4 == 0) ? 4 : 2));
-    stockham_pass<LEN, NSEQ, SSTRIDE, T, SIGN, NS, R>(buf, roots);
-    stockham_passes<LEN, NSEQ, SSTRIDE, T, SIGN, NS * R>(buf, roots);
+    constexpr int R = plan_radix(LEN / NS);
+    stockham_pass<LEN, NSEQ, SSTRIDE, T, SIGN, NS, R>(buf, twt);
+    stockham_passes<LEN, NSEQ, SSTRIDE, T, SIGN, NS * R>(buf, twt);
   }
 }
 
 // In-place FFT (natural order in and out) of NSEQ sequences of power-of-two length LEN
-// held at buf[seq*SSTRIDE + pidx(i)] (SSTRIDE >= padlen(LEN)).  Must be called by all T
-// threads of the block; the caller synchronises before (the inputs are visible); the
-// function ends with a barrier.
+// held at buf[seq*SSTRIDE + pidx(i)] (SSTRIDE >= padlen(LEN)).  twt: the length's
+// twiddle table (tw_size(LEN) entries, see tw_offset).  Must be called by all T threads of
+// the block; the caller synchronises before (the inputs are visible); the function ends
+// with a barrier.
 template <int LEN, int NSEQ, int SSTRIDE, int T, int SIGN>
-__device__ __forceinline__ void smem_fft(float2* buf, const float2* roots) {
+__device__ __forceinline__ void smem_fft(float2* buf, const float2* twt) {
   static_assert((LEN & (LEN - 1)) == 0, "power-of-two length");
   static_assert(SSTRIDE >= padlen(LEN), "sequence stride too small");
-  stockham_passes<LEN, NSEQ, SSTRIDE, T, SIGN, 1>(buf, roots);
+  stockham_passes<LEN, NSEQ, SSTRIDE, T, SIGN, 1>(buf, twt);
 }
 
 }  // namespace fdr

@@ -54,8 +54,8 @@ struct PhaseInt {
 };
 
 struct FusedTables {
-  const float2* rootsP;  // exp(-2 pi i m / P), m < P
-  const float2* rootsQ;  // exp(-2 pi i m / Q), m < Q
+  const float2* twP;     // Stockham pass twiddles of length P (tw_offset layout)
+  const float2* twQ;     // Stockham pass twiddles of length Q
   const float2* tw_lo;   // exp(-2 pi i m / N), m < 2^B
   const float2* tw_hi;   // exp(-2 pi i m 2^B / N), m < N / 2^B
   int B;
@@ -81,29 +81,32 @@ __global__ void __launch_bounds__(T)
 zdtf_input_kernel(const float* __restrict__ spec, long long N, int Nt, int Q,
                   float2* __restrict__ A, FusedTables tab) {
   constexpr int SS = ac_stride<P, TA>();
+  constexpr int TP = TA / 2;  // sequence pairs: each thread moves two adjacent channels
   extern __shared__ float2 sm[];
   float2* buf = sm;
-  float2* roots = sm + TA * SS;
+  float2* twt = sm + TA * SS;
   const int na0 = blockIdx.x * TA;
   const int p = blockIdx.y;
-  for (int i = threadIdx.x; i < P; i += T) roots[i] = __ldg(tab.rootsP + i);
+  for (int i = threadIdx.x; i < tw_size(P); i += T) twt[i] = __ldg(tab.twP + i);
   const float* c0 = spec + (long long)(2 * p) * N;
   const bool has1 = (2 * p + 1) < Nt;
   const float* c1 = spec + (long long)(2 * p + 1) * N;
-  for (int e = threadIdx.x; e < TA * P; e += T) {
-    const int seq = e % TA, nb = e / TA;
-    const long long n = (long long)(na0 + seq) + (long long)Q * nb;
-    const float a = __ldcs(c0 + n);
-    const float b = has1 ? __ldcs(c1 + n) : 0.f;
-    buf[seq * SS + pidx(nb)] = make_float2(a, b);
+  for (int e = threadIdx.x; e < TP * P; e += T) {
+    const int sp = e % TP, nb = e / TP;
+    const long long n = (long long)(na0 + 2 * sp) + (long long)Q * nb;
+    const float2 a = __ldcs(reinterpret_cast<const float2*>(c0 + n));
+    const float2 b = has1 ? __ldcs(reinterpret_cast<const float2*>(c1 + n)) : make_float2(0.f, 0.f);
+    buf[(2 * sp) * SS + pidx(nb)] = make_float2(a.x, b.x);
+    buf[(2 * sp + 1) * SS + pidx(nb)] = make_float2(a.y, b.y);
   }
   __syncthreads();
-  smem_fft<P, TA, SS, T, -1>(buf, roots);
-  for (int e = threadIdx.x; e < TA * P; e += T) {
-    const int seq = e % TA, k1 = e / TA;
-    const int na = na0 + seq;
-    const float2 w = tw_fwd(tab, (long long)k1 * na);
-    A[((long long)p * P + k1) * Q + na] = cmul(buf[seq * SS + pidx(k1)], w);
+  smem_fft<P, TA, SS, T, -1>(buf, twt);
+  for (int e = threadIdx.x; e < TP * P; e += T) {
+    const int sp = e % TP, k1 = e / TP;
+    const int na = na0 + 2 * sp;
+    const float2 v0 = cmul(buf[(2 * sp) * SS + pidx(k1)], tw_fwd(tab, (long long)k1 * na));
+    const float2 v1 = cmul(buf[(2 * sp + 1) * SS + pidx(k1)], tw_fwd(tab, (long long)k1 * (na + 1)));
+    *reinterpret_cast<float4*>(A + ((long long)p * P + k1) * Q + na) = make_float4(v0.x, v0.y, v1.x, v1.y);
   }
 }
 
@@ -133,7 +136,7 @@ __device__ __forceinline__ void mirror_of(int c, int side, int k2, int Q, int* m
 // F[N/2, t] into gnyq (shared memory).  buf holds 8 sequences of stride b_stride<Q>().
 template <int Q, int NTR>
 __device__ __forceinline__ void czt_forward(const CztArgs& a, int c, const int* k1s, float2* buf,
-                                            const float2* roots, float2* gnyq,
+                                            const float2* twt, float2* gnyq,
                                             float2 (&G)[2][NTR]) {
   constexpr int T = Q / 2;
   constexpr int SS = b_stride<Q>();
@@ -158,7 +161,7 @@ __device__ __forceinline__ void czt_forward(const CztArgs& a, int c, const int* 
         buf[seq * SS + pidx(na)] = v;
       }
       __syncthreads();
-      smem_fft<Q, 2 * PC, SS, T, -1>(buf, roots);
+      smem_fft<Q, 2 * PC, SS, T, -1>(buf, twt);
 #pragma unroll
       for (int b = 0; b < 2; ++b) {
         int ms, mk2;
@@ -213,22 +216,22 @@ __global__ void __launch_bounds__(Q / 2, 1) zdtf_czt_kernel(CztArgs a) {
   constexpr int T = Q / 2;
   constexpr int SS = b_stride<Q>();
   extern __shared__ float2 sm[];
-  float2* buf = sm;                // kRatesPerBlock * SS
-  float2* roots = buf + kRatesPerBlock * SS;  // Q
-  float2* twr = roots + Q;         // 2 * Q
-  float2* gnyq = twr + 2 * Q;      // NTR
+  float2* buf = sm;                           // kRatesPerBlock * SS
+  float2* twt = buf + kRatesPerBlock * SS;    // tw_size(Q)
+  float2* twr = twt + tw_size(Q);             // 2 * Q
+  float2* gnyq = twr + 2 * Q;                 // NTR
   const int tid = threadIdx.x;
   const int c = blockIdx.x;
   const int P = a.P;
   const int k1s[2] = {c == 0 ? 0 : c, c == 0 ? P / 2 : P - c};
   const float invN = 1.0f / (float)a.N;
-  for (int i = tid; i < Q; i += T) roots[i] = __ldg(a.tab.rootsQ + i);
+  for (int i = tid; i < tw_size(Q); i += T) twt[i] = __ldg(a.tab.twQ + i);
   for (int i = tid; i < 2 * Q; i += T) {
     const int side = i / Q, na = i - side * Q;
     twr[i] = cscale(cconj(tw_fwd(a.tab, (long long)k1s[side] * na)), invN);
   }
   float2 G[2][NTR];
-  czt_forward<Q, NTR>(a, c, k1s, buf, roots, gnyq, G);
+  czt_forward<Q, NTR>(a, c, k1s, buf, twt, gnyq, G);
 
   // Per-base phase state: w_{k,j} = exp(2 pi i (alpha + j*beta) / 2^bits); rates are taken
   // kHorner at a time, w = w(first rate of the group, exact) * pw[jr] (exact).
@@ -307,12 +310,16 @@ __global__ void __launch_bounds__(Q / 2, 1) zdtf_czt_kernel(CztArgs a) {
       }
     }
     __syncthreads();
-    smem_fft<Q, kRatesPerBlock, SS, T, +1>(buf, roots);
-    for (int e = tid; e < kRatesPerBlock * Q; e += T) {
-      const int seq = e / Q, na = e - seq * Q;
+    smem_fft<Q, kRatesPerBlock, SS, T, +1>(buf, twt);
+    for (int e = tid; e < kRatesPerBlock * Q / 2; e += T) {
+      const int seq = e / (Q / 2), na = 2 * (e - seq * (Q / 2));
       const int q = q0 + (seq >> 1), side = seq & 1;
-      if (q < q_end)
-        a.W[((long long)q * P + k1s[side]) * Q + na] = cmul(buf[seq * SS + pidx(na)], twr[side * Q + na]);
+      if (q < q_end) {
+        const float2 v0 = cmul(buf[seq * SS + pidx(na)], twr[side * Q + na]);
+        const float2 v1 = cmul(buf[seq * SS + pidx(na + 1)], twr[side * Q + na + 1]);
+        *reinterpret_cast<float4*>(a.W + ((long long)q * P + k1s[side]) * Q + na) =
+            make_float4(v0.x, v0.y, v1.x, v1.y);
+      }
     }
   }
 }
@@ -324,17 +331,16 @@ __global__ void __launch_bounds__(Q / 2, 1) zdtf_a2f_kernel(CztArgs a) {
   constexpr int SS = b_stride<Q>();
   extern __shared__ float2 sm[];
   float2* buf = sm;
-  float2* roots = buf + kRatesPerBlock * SS;
-  float2* twr = roots + Q;
+  float2* twt = buf + kRatesPerBlock * SS;
+  float2* twr = twt + tw_size(Q);
   float2* gnyq = twr + 2 * Q;
   const int tid = threadIdx.x;
   const int c = blockIdx.x;
   const int P = a.P;
   const int k1s[2] = {c == 0 ? 0 : c, c == 0 ? P / 2 : P - c};
-  for (int i = tid; i < Q; i += T) roots[i] = __ldg(a.tab.rootsQ + i);
-  (void)twr;
+  for (int i = tid; i < tw_size(Q); i += T) twt[i] = __ldg(a.tab.twQ + i);
   float2 G[2][NTR];
-  czt_forward<Q, NTR>(a, c, k1s, buf, roots, gnyq, G);
+  czt_forward<Q, NTR>(a, c, k1s, buf, twt, gnyq, G);
   const long long K = a.N / 2 + 1;
 #pragma unroll
   for (int b = 0; b < 2; ++b) {
@@ -356,29 +362,33 @@ __global__ void __launch_bounds__(T)
 zdtf_output_kernel(const float2* __restrict__ W, long long N, int Q, int Nr, float* __restrict__ dest,
                    FusedTables tab) {
   constexpr int SS = ac_stride<P, TC>();
+  constexpr int TP = TC / 2;
   extern __shared__ float2 sm[];
   float2* buf = sm;
-  float2* roots = sm + TC * SS;
+  float2* twt = sm + TC * SS;
   const int na0 = blockIdx.x * TC;
   const int q = blockIdx.y;
-  for (int i = threadIdx.x; i < P; i += T) roots[i] = __ldg(tab.rootsP + i);
+  for (int i = threadIdx.x; i < tw_size(P); i += T) twt[i] = __ldg(tab.twP + i);
   const float2* w = W + (long long)q * P * Q;
-  for (int e = threadIdx.x; e < TC * P; e += T) {
-    const int seq = e % TC, k1 = e / TC;
-    buf[seq * SS + pidx(k1)] = __ldcs(w + (long long)k1 * Q + na0 + seq);
+  for (int e = threadIdx.x; e < TP * P; e += T) {
+    const int sp = e % TP, k1 = e / TP;
+    const float4 v = __ldcs(reinterpret_cast<const float4*>(w + (long long)k1 * Q + na0 + 2 * sp));
+    buf[(2 * sp) * SS + pidx(k1)] = make_float2(v.x, v.y);
+    buf[(2 * sp + 1) * SS + pidx(k1)] = make_float2(v.z, v.w);
   }
   __syncthreads();
-  smem_fft<P, TC, SS, T, +1>(buf, roots);
+  smem_fft<P, TC, SS, T, +1>(buf, twt);
   const int j = 2 * q;
   float* d0 = dest + (long long)j * N;
   float* d1 = dest + (long long)(j + 1) * N;
   const bool has1 = (j + 1) < Nr;
-  for (int e = threadIdx.x; e < TC * P; e += T) {
-    const int seq = e % TC, nb = e / TC;
-    const long long n = (long long)(na0 + seq) + (long long)Q * nb;
-    const float2 v = buf[seq * SS + pidx(nb)];
-    __stcs(d0 + n, v.x);
-    if (has1) __stcs(d1 + n, v.y);
+  for (int e = threadIdx.x; e < TP * P; e += T) {
+    const int sp = e % TP, nb = e / TP;
+    const long long n = (long long)(na0 + 2 * sp) + (long long)Q * nb;
+    const float2 v0 = buf[(2 * sp) * SS + pidx(nb)];
+    const float2 v1 = buf[(2 * sp + 1) * SS + pidx(nb)];
+    __stcs(reinterpret_cast<float2*>(d0 + n), make_float2(v0.x, v1.x));
+    if (has1) __stcs(reinterpret_cast<float2*>(d1 + n), make_float2(v0.y, v1.y));
   }
 }
 
@@ -391,12 +401,13 @@ template <int P>
 struct AcShape {
   static constexpr int TILE = P >= 4096 ? 4 : 8;
   static constexpr int T = (TILE * P / 16 > 512) ? 512 : (TILE * P / 16 < 32 ? 32 : TILE * P / 16);
-  static constexpr size_t SMEM = sizeof(float2) * (TILE * ac_stride<P, TILE>() + P);
+  static constexpr size_t SMEM = sizeof(float2) * (TILE * ac_stride<P, TILE>() + tw_size(P));
 };
 
 template <int Q>
 struct CztShape {
-  static constexpr size_t SMEM = sizeof(float2) * (kRatesPerBlock * b_stride<Q>() + 3 * Q + kFusedMaxNt);
+  static constexpr size_t SMEM =
+      sizeof(float2) * (kRatesPerBlock * b_stride<Q>() + tw_size(Q) + 2 * Q + kFusedMaxNt);
 };
 
 bool zdt_fused_eligible(int64_t Nf, int64_t Nt, int64_t Nr) {
@@ -444,7 +455,7 @@ static bool make_phase(float r0, float dr, int L, PhaseInt* ph) {
 
 struct FusedState {
   int L, B;
-  float2* tables = nullptr;  // rootsP | rootsQ | tw_lo | tw_hi
+  float2* tables = nullptr;  // twP | twQ | tw_lo | tw_hi
   FusedTables tab;
   int64_t NP = 0, npairs = 0;
 };
@@ -456,6 +467,26 @@ static std::vector<float2> roots_table(long long n, long long N, long long count
     const long long r = (m * n) % N;
     const double a = -2.0 * (double)r / (double)N;  // half-turns in (-2, 0]
     h[(size_t)m] = make_float2((float)cos(M_PI * a), (float)sin(M_PI * a));
+  }
+  return h;
+}
+
+// Stockham pass twiddles for length len in the tw_offset layout.
+static std::vector<float2> pass_twiddles(int len) {
+  std::vector<float2> h((size_t)tw_size(len));
+  int ns = 1;
+  while (ns < len) {
+    const int R = plan_radix(len / ns);
+    if (ns > 1) {
+      const int off = tw_offset(len, ns);
+      for (int r = 1; r < R; ++r)
+        for (int k = 0; k < ns; ++k) {
+          const long long m = (long long)r * k, M = (long long)ns * R;
+          const double a = -2.0 * (double)(m % M) / (double)M;
+          h[(size_t)(off + (r - 1) * ns + k)] = make_float2((float)cos(M_PI * a), (float)sin(M_PI * a));
+        }
+    }
+    ns *= R;
   }
   return h;
 }
@@ -501,22 +532,23 @@ int zdt_fused_setup(fdr_zdt* ws) {
   ws->fstate = st;
   const long long N = ws->Nf, P = ws->fP, Q = ws->fQ;
   const long long nlo = 1LL << st->B, nhi = N >> st->B;
-  const long long ntab = P + Q + nlo + nhi;
+  const long long ntwP = tw_size((int)P), ntwQ = tw_size((int)Q);
+  const long long ntab = ntwP + ntwQ + nlo + nhi;
   FDR_TRY(set_smem_attrs());
   cudaError_t e;
   if ((e = cudaMalloc(&st->tables, sizeof(float2) * ntab)) != cudaSuccess) return cuda_status(e, "cudaMalloc(fused tables)");
   std::vector<float2> h;
   auto append = [&](const std::vector<float2>& v) { h.insert(h.end(), v.begin(), v.end()); };
-  append(roots_table(1, P, P));
-  append(roots_table(1, Q, Q));
+  append(pass_twiddles((int)P));
+  append(pass_twiddles((int)Q));
   append(roots_table(1, N, nlo));
   append(roots_table(nlo, N, nhi));
   if ((e = cudaMemcpy(st->tables, h.data(), sizeof(float2) * ntab, cudaMemcpyHostToDevice)) != cudaSuccess)
     return cuda_status(e, "upload fused tables");
-  st->tab.rootsP = st->tables;
-  st->tab.rootsQ = st->tables + P;
-  st->tab.tw_lo = st->tables + P + Q;
-  st->tab.tw_hi = st->tables + P + Q + nlo;
+  st->tab.twP = st->tables;
+  st->tab.twQ = st->tables + ntwP;
+  st->tab.tw_lo = st->tables + ntwP + ntwQ;
+  st->tab.tw_hi = st->tables + ntwP + ntwQ + nlo;
   st->tab.B = st->B;
   if ((e = cudaMalloc(&ws->A, sizeof(float2) * N * st->NP)) != cudaSuccess) return cuda_status(e, "cudaMalloc(A)");
   ws->W_pairs = st->npairs;
