@@ -95,6 +95,7 @@ SIGNATURES = {
     "fdr_fdshift": (INT, [P, F32, P, P]),
     "fdr_fftfdr": (INT, [P, C.POINTER(F32), I64, P, P]),
     "fdr_stats": (INT, [C.POINTER(P), I64, I64, I64, C.POINTER(F64), C.POINTER(F64), P]),
+    "fdr_stats_noalloc": (INT, [P, I64, I64, C.POINTER(F64), C.POINTER(F64), P]),
     "fdr_normalize": (INT, [C.POINTER(P), I64, I64, I64, F32, F32, P]),
     "fdr_findprotohits": (INT, [C.POINTER(P), I64, I64, I64, F64, INT, P, I64,
                                 C.POINTER(I64), C.POINTER(F64), P]),

@@ -193,6 +193,22 @@ int fdr_fftfdr(fdr_fft_ws* ws, const float* rates, int64_t Nr, float* fdr,
    float64.  Synchronises `stream` and writes host doubles. */
 int fdr_stats(const float* const* fdrs, int64_t nb, int64_t Nf, int64_t Nrb, double* m,
               double* s, fdr_stream_t stream);
+/* fdrstats of a single FDR matrix without allocating device memory.  This entry point has
+   no counterpart in the reference; it serves callers that must not allocate once they are
+   running -- e.g. a real-time pipeline (an allocation can stall on the device or fail when
+   memory is short) or a host whose device memory is entirely held by its own pool
+   allocator.  Same results as fdr_stats for nb = 1 (float64 accumulation; the summation
+   order may differ in the last bits).  Its scratch space is a fixed file-scope device array
+   sized for at most FDR_STATS_NOALLOC_MAX_COLUMNS columns (16 bytes per column plus 16),
+   which every GPU that loads the library keeps until the process exits; larger Nr is
+   rejected with FDR_ERR_INVALID_ARGUMENT.  All calls share that array: calls whose work
+   overlaps on the GPU (different streams or devices' threads racing on one device) race,
+   so serialise them.  The first call on a device looks up the array's device address
+   (cudaGetSymbolAddress) with that device current; make that first call before any stream
+   capture.  Synchronises `stream` and writes host doubles. */
+#define FDR_STATS_NOALLOC_MAX_COLUMNS 8192
+int fdr_stats_noalloc(const float* fdr, int64_t Nf, int64_t Nr, double* m, double* s,
+                      fdr_stream_t stream);
 /* fdrnormalize! (fdrutils.jl:70-90): x = (x - m) / s in float32 for nb matrices. */
 int fdr_normalize(float* const* fdrs, int64_t nb, int64_t Nf, int64_t Nrb, float m, float s,
                   fdr_stream_t stream);
