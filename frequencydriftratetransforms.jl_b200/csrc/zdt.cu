@@ -130,8 +130,11 @@ void zdt_mark(fdr_zdt* ws, const char* name, cudaStream_t s) {
   ws->ev_names.push_back(name);
 }
 
+static int zdt_ensure_staged(fdr_zdt* ws, cudaStream_t s);
+
 int zdt_stage_input(fdr_zdt* ws, const float* spec, cudaStream_t s) {
   FDR_CHECK_ARG(spec != nullptr, "input!: spectrogram is NULL");
+  FDR_TRY(zdt_ensure_staged(ws, s));
   FDR_TRY(rfft_columns(spec, ws->Nf, ws->Nt, ws->Nf, ws->F, ws->K, ws->rscratch,
                        ws->rscratch_pairs, s));
   ws->F_valid = true;
@@ -152,7 +155,32 @@ int zdt_ensure_F(fdr_zdt* ws, cudaStream_t s) {
   return FDR_OK;
 }
 
+static int zdt_compute_V(fdr_zdt* ws, cudaStream_t s);
+
+// Y, V and the real-FFT scratch of the staged stages.  Workspaces that run zdtfdr! on the
+// fused kernels allocate them (and compute V) on the first staged call only.
+static int zdt_ensure_staged(fdr_zdt* ws, cudaStream_t s) {
+  if (ws->Y && ws->V && ws->rscratch) return FDR_OK;
+  const int64_t K = ws->K, Nl = ws->Nl;
+  const int64_t per = real_fft_scratch_per_pair(ws->Nf);
+  if (!ws->Y) {
+    FDR_CUDA(cudaMalloc(&ws->Y, sizeof(float2) * K * Nl));
+    ws->bytes += (int64_t)sizeof(float2) * K * Nl;
+  }
+  if (!ws->rscratch) {
+    FDR_CUDA(cudaMalloc(&ws->rscratch, sizeof(float2) * per * ws->rscratch_pairs));
+    ws->bytes += (int64_t)sizeof(float2) * per * ws->rscratch_pairs;
+  }
+  if (!ws->V) {
+    FDR_CUDA(cudaMalloc(&ws->V, sizeof(float2) * K * Nl));
+    ws->bytes += (int64_t)sizeof(float2) * K * Nl;
+    FDR_TRY(zdt_compute_V(ws, s));
+  }
+  return FDR_OK;
+}
+
 static int zdt_preprocess(fdr_zdt* ws, float r0, cudaStream_t s) {
+  FDR_TRY(zdt_ensure_staged(ws, s));
   FDR_TRY(zdt_ensure_F(ws, s));
   zdt_preprocess_kernel<<<grid_1d(ws->K * ws->Nl), 256, 0, s>>>(
       ws->F, ws->Y, ws->K, ws->Nt, ws->Nl, ws->Nf, r0, ws->dr,
@@ -162,6 +190,7 @@ static int zdt_preprocess(fdr_zdt* ws, float r0, cudaStream_t s) {
 }
 
 static int zdt_convolve(fdr_zdt* ws, cudaStream_t s) {
+  FDR_TRY(zdt_ensure_staged(ws, s));
   FDR_TRY(fft_strided_inplace(ws->Y, ws->Nl, ws->K, ws->K, 1, -1, 1.f, ws->V, s));
   FDR_TRY(fft_strided_inplace(ws->Y, ws->Nl, ws->K, ws->K, 1, +1, 1.f / (float)ws->Nl, nullptr, s));
   return FDR_OK;
@@ -174,6 +203,7 @@ static int zdt_postprocess(fdr_zdt* ws, int window, const double* wk, cudaStream
   }
   FDR_CHECK_ARG(window != FDR_WINDOW_CUSTOM || wk != nullptr,
                 "postprocess!: custom window values are NULL");
+  FDR_TRY(zdt_ensure_staged(ws, s));
   zdt_postprocess_kernel<<<grid_1d(ws->K * ws->Nr), 256, 0, s>>>(
       ws->Y, ws->K, ws->Nr, ws->Nf, ws->dr, (ws->flags & FDR_ZDT_EXACT_PHASE) ? 1 : 0, window, wk);
   FDR_LAUNCH_CHECK("zdt_postprocess_kernel");
@@ -182,6 +212,7 @@ static int zdt_postprocess(fdr_zdt* ws, int window, const double* wk, cudaStream
 
 static int zdt_output(fdr_zdt* ws, float* dest, cudaStream_t s) {
   FDR_CHECK_ARG(dest != nullptr, "output!: dest is NULL");
+  FDR_TRY(zdt_ensure_staged(ws, s));
   return irfft_columns(ws->Y, ws->K, ws->Nr, ws->Nf, dest, ws->Nf, ws->rscratch,
                        ws->rscratch_pairs, s);
 }
@@ -277,18 +308,16 @@ int fdr_zdt_create(fdr_zdt** out, const float* spectrogram, int64_t Nf, int64_t 
   };
   cudaError_t e;
   if ((e = cudaMalloc(&ws->F, sizeof(float2) * K * Nt)) != cudaSuccess) return fail(e, "cudaMalloc(F)");
-  if ((e = cudaMalloc(&ws->Y, sizeof(float2) * K * Nl)) != cudaSuccess) return fail(e, "cudaMalloc(Y)");
-  if ((e = cudaMalloc(&ws->V, sizeof(float2) * K * Nl)) != cudaSuccess) return fail(e, "cudaMalloc(V)");
-  if ((e = cudaMalloc(&ws->rscratch, sizeof(float2) * per * ws->rscratch_pairs)) != cudaSuccess)
-    return fail(e, "cudaMalloc(fft scratch)");
-  ws->bytes = (int64_t)sizeof(float2) * (K * Nt + 2 * K * Nl + per * ws->rscratch_pairs);
-  if (!(flags & FDR_ZDT_STAGED_ONLY) && zdt_fused_eligible(Nf, Nt, Nr)) {
-    int st = zdt_fused_setup(ws);
-    if (st != FDR_OK) { release(ws); return st; }
-  }
+  ws->bytes = (int64_t)sizeof(float2) * K * Nt;
+  (void)per;
   int st = FDR_OK;
+  if (!(flags & FDR_ZDT_STAGED_ONLY) && zdt_fused_eligible(Nf, Nt, Nr)) {
+    st = zdt_fused_setup(ws);
+  } else {
+    st = zdt_ensure_staged(ws, s);  // allocates Y, V, scratch and computes V (computeV!)
+  }
+  if (st != FDR_OK) { release(ws); return st; }
   if (spectrogram) st = fdr_zdt_input(ws, spectrogram, stream);
-  if (st == FDR_OK) st = zdt_compute_V(ws, s);
   if (st == FDR_OK) {
     e = s ? cudaStreamSynchronize(s) : cudaDeviceSynchronize();
     if (e != cudaSuccess) st = cuda_status(e, "ZDTWorkspace synchronize");
@@ -324,6 +353,10 @@ int fdr_zdt_buffers(fdr_zdt* ws, void** F, void** Y, void** V) {
     FDR_TRY(zdt_ensure_F(ws, nullptr));
     FDR_CUDA(cudaDeviceSynchronize());
     *F = ws->F;
+  }
+  if (Y || V) {
+    FDR_TRY(zdt_ensure_staged(ws, nullptr));
+    FDR_CUDA(cudaDeviceSynchronize());
   }
   if (Y) *Y = ws->Y;
   if (V) *V = ws->V;

@@ -91,13 +91,25 @@ zdtf_input_kernel(const float* __restrict__ spec, long long N, int Nt, int Q,
   const float* c0 = spec + (long long)(2 * p) * N;
   const bool has1 = (2 * p + 1) < Nt;
   const float* c1 = spec + (long long)(2 * p + 1) * N;
-  for (int e = threadIdx.x; e < TP * P; e += T) {
-    const int sp = e % TP, nb = e / TP;
-    const long long n = (long long)(na0 + 2 * sp) + (long long)Q * nb;
-    const float2 a = __ldcs(reinterpret_cast<const float2*>(c0 + n));
-    const float2 b = has1 ? __ldcs(reinterpret_cast<const float2*>(c1 + n)) : make_float2(0.f, 0.f);
-    buf[(2 * sp) * SS + pidx(nb)] = make_float2(a.x, b.x);
-    buf[(2 * sp + 1) * SS + pidx(nb)] = make_float2(a.y, b.y);
+  static_assert((TP * P) % T == 0, "tile must divide evenly");
+  constexpr int NL = TP * P / T;  // loads per thread: all issued before any is consumed
+  {
+    float2 a[NL], b[NL];
+#pragma unroll
+    for (int i = 0; i < NL; ++i) {
+      const int e = threadIdx.x + i * T;
+      const int sp = e % TP, nb = e / TP;
+      const long long n = (long long)(na0 + 2 * sp) + (long long)Q * nb;
+      a[i] = __ldcs(reinterpret_cast<const float2*>(c0 + n));
+      b[i] = has1 ? __ldcs(reinterpret_cast<const float2*>(c1 + n)) : make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int i = 0; i < NL; ++i) {
+      const int e = threadIdx.x + i * T;
+      const int sp = e % TP, nb = e / TP;
+      buf[(2 * sp) * SS + pidx(nb)] = make_float2(a[i].x, b[i].x);
+      buf[(2 * sp + 1) * SS + pidx(nb)] = make_float2(a[i].y, b[i].y);
+    }
   }
   __syncthreads();
   smem_fft<P, TA, SS, T, -1>(buf, twt);
@@ -153,12 +165,23 @@ __device__ __forceinline__ void czt_forward(const CztArgs& a, int c, const int* 
   for (int p0 = 0; p0 < NTR / 2; p0 += PC) {
     if (p0 < a.NP) {
       __syncthreads();
-      for (int e = tid; e < 2 * PC * Q; e += T) {
-        const int seq = e / Q, na = e - seq * Q;
-        const int pp = p0 + (seq >> 1), side = seq & 1;
-        float2 v = make_float2(0.f, 0.f);
-        if (pp < a.NP) v = a.A[((long long)pp * a.P + k1s[side]) * Q + na];
-        buf[seq * SS + pidx(na)] = v;
+      {
+        constexpr int NL = 2 * PC * Q / T;  // loads per thread, issued before any is stored
+        float2 v[NL];
+#pragma unroll
+        for (int i = 0; i < NL; ++i) {
+          const int e = tid + i * T;
+          const int seq = e / Q, na = e - seq * Q;
+          const int pp = p0 + (seq >> 1), side = seq & 1;
+          v[i] = (pp < a.NP) ? __ldcs(a.A + ((long long)pp * a.P + k1s[side]) * Q + na)
+                             : make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int i = 0; i < NL; ++i) {
+          const int e = tid + i * T;
+          const int seq = e / Q, na = e - seq * Q;
+          buf[seq * SS + pidx(na)] = v[i];
+        }
       }
       __syncthreads();
       smem_fft<Q, 2 * PC, SS, T, -1>(buf, twt);
@@ -370,11 +393,23 @@ zdtf_output_kernel(const float2* __restrict__ W, long long N, int Q, int Nr, flo
   const int q = blockIdx.y;
   for (int i = threadIdx.x; i < tw_size(P); i += T) twt[i] = __ldg(tab.twP + i);
   const float2* w = W + (long long)q * P * Q;
-  for (int e = threadIdx.x; e < TP * P; e += T) {
-    const int sp = e % TP, k1 = e / TP;
-    const float4 v = __ldcs(reinterpret_cast<const float4*>(w + (long long)k1 * Q + na0 + 2 * sp));
-    buf[(2 * sp) * SS + pidx(k1)] = make_float2(v.x, v.y);
-    buf[(2 * sp + 1) * SS + pidx(k1)] = make_float2(v.z, v.w);
+  static_assert((TP * P) % T == 0, "tile must divide evenly");
+  constexpr int NL = TP * P / T;  // loads per thread: all issued before any is consumed
+  {
+    float4 v[NL];
+#pragma unroll
+    for (int i = 0; i < NL; ++i) {
+      const int e = threadIdx.x + i * T;
+      const int sp = e % TP, k1 = e / TP;
+      v[i] = __ldcs(reinterpret_cast<const float4*>(w + (long long)k1 * Q + na0 + 2 * sp));
+    }
+#pragma unroll
+    for (int i = 0; i < NL; ++i) {
+      const int e = threadIdx.x + i * T;
+      const int sp = e % TP, k1 = e / TP;
+      buf[(2 * sp) * SS + pidx(k1)] = make_float2(v[i].x, v[i].y);
+      buf[(2 * sp + 1) * SS + pidx(k1)] = make_float2(v[i].z, v[i].w);
+    }
   }
   __syncthreads();
   smem_fft<P, TC, SS, T, +1>(buf, twt);
