@@ -96,6 +96,42 @@ struct Dft<16> {
 };
 
 template <>
+struct Dft<32> {
+  // radix-2 split into even / odd halves, each a 16-point DFT
+  __device__ __forceinline__ static void run(float2* v, int sign) {
+    // cos / sin of 2*pi*m/32, m = 0..15
+    const float C[16] = {1.f, 0.98078528040323044913f, 0.92387953251128675613f,
+                         0.83146961230254523708f, 0.70710678118654752440f,
+                         0.55557023301960222474f, 0.38268343236508977173f,
+                         0.19509032201612826785f, 0.f, -0.19509032201612826785f,
+                         -0.38268343236508977173f, -0.55557023301960222474f,
+                         -0.70710678118654752440f, -0.83146961230254523708f,
+                         -0.92387953251128675613f, -0.98078528040323044913f};
+    const float S[16] = {0.f, 0.19509032201612826785f, 0.38268343236508977173f,
+                         0.55557023301960222474f, 0.70710678118654752440f,
+                         0.83146961230254523708f, 0.92387953251128675613f,
+                         0.98078528040323044913f, 1.f, 0.98078528040323044913f,
+                         0.92387953251128675613f, 0.83146961230254523708f,
+                         0.70710678118654752440f, 0.55557023301960222474f,
+                         0.38268343236508977173f, 0.19509032201612826785f};
+    float2 e[16], o[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      e[i] = v[2 * i];
+      o[i] = v[2 * i + 1];
+    }
+    Dft<16>::run(e, sign);
+    Dft<16>::run(o, sign);
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+      const float2 t = (m == 0) ? o[0] : cmul(o[m], make_float2(C[m], sign * S[m]));
+      v[m] = cadd(e[m], t);
+      v[m + 16] = csub(e[m], t);
+    }
+  }
+};
+
+template <>
 struct Dft<3> {
   __device__ __forceinline__ static void run(float2* v, int sign) {
     const float c = -0.5f, sn = 0.86602540378443864676f;

@@ -54,6 +54,7 @@ struct PhaseInt {
 };
 
 struct FusedTables {
+  const float2* rootsP;  // exp(-2 pi i m / P), m < P
   const float2* twP;     // Stockham pass twiddles of length P (tw_offset layout)
   const float2* twQ;     // Stockham pass twiddles of length Q
   const float2* tw_lo;   // exp(-2 pi i m / N), m < 2^B
@@ -427,6 +428,69 @@ zdtf_output_kernel(const float2* __restrict__ W, long long N, int Q, int Nr, flo
   }
 }
 
+// Kernel C for P = P1 * P2 (P1, P2 in {8, 16, 32}): two register passes with one
+// shared-memory transpose.  k1 = k1a + P1*k1b, nb = nb_b + P2*nb_a:
+//   z[nb_b + P2*nb_a] = sum_k1a w_P1^(k1a*nb_a) * w_P^(k1a*nb_b) * sum_k1b X[k1a + P1*k1b] w_P2^(k1b*nb_b)
+// Thread (seq, k1a) loads its P2 inputs straight from W, transforms them in registers,
+// applies the twiddle and writes them transposed; thread (seq, nb_b) then transforms over
+// k1a and writes its P1 outputs (two rates of the pair) to the FDR columns.
+template <int P1, int P2, int TS>
+struct Out2Shape {
+  static constexpr int P = P1 * P2;
+  static constexpr int T = TS * (P1 > P2 ? P1 : P2);
+  static constexpr int S1 = P2 + 1;                       // k1a stride (float2)
+  static constexpr int SSEQ = ((P1 * S1 + 15) / 16) * 16 + 2;  // sequence stride, = 2 mod 16
+  static constexpr size_t SMEM = sizeof(float2) * (TS * SSEQ + P);
+};
+
+template <int P1, int P2, int TS>
+__global__ void __launch_bounds__(Out2Shape<P1, P2, TS>::T)
+zdtf_output2_kernel(const float2* __restrict__ W, long long N, int Q, int Nr,
+                    float* __restrict__ dest, const float2* __restrict__ rootsP) {
+  using SH = Out2Shape<P1, P2, TS>;
+  constexpr int P = SH::P, S1 = SH::S1, SSEQ = SH::SSEQ;
+  extern __shared__ float2 sm[];
+  float2* buf = sm;
+  float2* roots = sm + TS * SSEQ;  // exp(-2 pi i m / P)
+  const int na0 = blockIdx.x * TS;
+  const int q = blockIdx.y;
+  for (int i = threadIdx.x; i < P; i += SH::T) roots[i] = __ldg(rootsP + i);
+  const int seq = threadIdx.x % TS;
+  const int r = threadIdx.x / TS;  // k1a in pass 1, nb_b in pass 2
+  const float2* w = W + (long long)q * P * Q + na0 + seq;
+  __syncthreads();
+  if (r < P1) {
+    float2 v[P2];
+#pragma unroll
+    for (int m = 0; m < P2; ++m) v[m] = __ldcs(w + (long long)(r + P1 * m) * Q);
+    Dft<P2>::run(v, +1);
+    float2* b = buf + seq * SSEQ + r * S1;
+#pragma unroll
+    for (int nbb = 0; nbb < P2; ++nbb) {
+      const float2 t = roots[(r * nbb) & (P - 1)];
+      b[nbb] = cmul(v[nbb], make_float2(t.x, -t.y));
+    }
+  }
+  __syncthreads();
+  if (r < P2) {
+    float2 v[P1];
+    const float2* b = buf + seq * SSEQ + r;
+#pragma unroll
+    for (int k1a = 0; k1a < P1; ++k1a) v[k1a] = b[k1a * S1];
+    Dft<P1>::run(v, +1);
+    const int j = 2 * q;
+    float* d0 = dest + (long long)j * N + na0 + seq + (long long)Q * r;
+    float* d1 = d0 + N;
+    const bool has1 = (j + 1) < Nr;
+#pragma unroll
+    for (int nba = 0; nba < P1; ++nba) {
+      const long long off = (long long)Q * P2 * nba;
+      __stcs(d0 + off, v[nba].x);
+      if (has1) __stcs(d1 + off, v[nba].y);
+    }
+  }
+}
+
 // ------------------------------------------------------------------------------------
 // Host side
 // ------------------------------------------------------------------------------------
@@ -541,6 +605,12 @@ static int set_smem_attrs() {
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)AcShape<P>::SMEM));
   FDR_FOR_P(SET_AC)
 #undef SET_AC
+#define SET_C2(P1, P2)                                                                         \
+  FDR_CUDA(cudaFuncSetAttribute(zdtf_output2_kernel<P1, P2, 8>,                                \
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,                   \
+                                (int)Out2Shape<P1, P2, 8>::SMEM));
+  SET_C2(8, 8) SET_C2(8, 16) SET_C2(16, 16) SET_C2(16, 32) SET_C2(32, 32)
+#undef SET_C2
 #define SET_B(Q)                                                                               \
   FDR_CUDA(cudaFuncSetAttribute(zdtf_czt_kernel<Q, kFusedMaxNt>,                               \
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CztShape<Q>::SMEM)); \
@@ -568,7 +638,7 @@ int zdt_fused_setup(fdr_zdt* ws) {
   const long long N = ws->Nf, P = ws->fP, Q = ws->fQ;
   const long long nlo = 1LL << st->B, nhi = N >> st->B;
   const long long ntwP = tw_size((int)P), ntwQ = tw_size((int)Q);
-  const long long ntab = ntwP + ntwQ + nlo + nhi;
+  const long long ntab = ntwP + ntwQ + nlo + nhi + P;
   FDR_TRY(set_smem_attrs());
   cudaError_t e;
   if ((e = cudaMalloc(&st->tables, sizeof(float2) * ntab)) != cudaSuccess) return cuda_status(e, "cudaMalloc(fused tables)");
@@ -578,12 +648,14 @@ int zdt_fused_setup(fdr_zdt* ws) {
   append(pass_twiddles((int)Q));
   append(roots_table(1, N, nlo));
   append(roots_table(nlo, N, nhi));
+  append(roots_table(1, P, P));
   if ((e = cudaMemcpy(st->tables, h.data(), sizeof(float2) * ntab, cudaMemcpyHostToDevice)) != cudaSuccess)
     return cuda_status(e, "upload fused tables");
   st->tab.twP = st->tables;
   st->tab.twQ = st->tables + ntwP;
   st->tab.tw_lo = st->tables + ntwP + ntwQ;
   st->tab.tw_hi = st->tables + ntwP + ntwQ + nlo;
+  st->tab.rootsP = st->tables + ntwP + ntwQ + nlo + nhi;
   st->tab.B = st->B;
   if ((e = cudaMalloc(&ws->A, sizeof(float2) * N * st->NP)) != cudaSuccess) return cuda_status(e, "cudaMalloc(A)");
   ws->W_pairs = st->npairs;
@@ -692,6 +764,21 @@ int zdt_fused_run(fdr_zdt* ws, float r0, float* dest, int window, const double* 
     return FDR_ERR_UNSUPPORTED_SIZE;
   }
   zdt_mark(ws, "czt", s);
+#define LAUNCH_C2(PP, P1, P2)                                                                  \
+  if (P == PP) {                                                                               \
+    using SH = Out2Shape<P1, P2, 8>;                                                           \
+    zdtf_output2_kernel<P1, P2, 8><<<dim3(Q / 8, (unsigned)st->npairs), SH::T, SH::SMEM, s>>>( \
+        ws->W, ws->Nf, Q, (int)ws->Nr, dest, st->tab.rootsP);                                  \
+    FDR_LAUNCH_CHECK("zdtf_output2_kernel");                                                   \
+    zdt_mark(ws, "output", s);                                                                 \
+    return FDR_OK;                                                                             \
+  }
+  LAUNCH_C2(64, 8, 8)
+  LAUNCH_C2(128, 8, 16)
+  LAUNCH_C2(256, 16, 16)
+  LAUNCH_C2(512, 16, 32)
+  LAUNCH_C2(1024, 32, 32)
+#undef LAUNCH_C2
 #define LAUNCH_C(PP)                                                                           \
   if (P == PP) {                                                                               \
     constexpr int TC = AcShape<PP>::TILE, T = AcShape<PP>::T;                                  \
