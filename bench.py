@@ -231,15 +231,14 @@ def main():
     nh_total = 0
     for i in range(2 if e2e_steps else 0):
         dev_in.t().copy_(pinned[i % nbuf], non_blocking=True)
-        fdr.zdtfdr_(dest, ws, dev_in)
-        fdr.findprotohits(dest, HIT_SNR, snr=True)
+        fdr.zdtfdr_protohits_(dest, ws, dev_in, threshold=HIT_SNR, snr=True)
     torch.cuda.synchronize()
     barrier()
     t0 = time.perf_counter()
     for i in range(e2e_steps):
         dev_in.t().copy_(pinned[i % nbuf], non_blocking=True)
-        fdr.zdtfdr_(dest, ws, dev_in)
-        hits = fdr.findprotohits(dest, HIT_SNR, snr=True)  # synchronises, copies hits to host
+        # zdtfdr! with the fused threshold/proto-hit scan; synchronises, hits copied to host
+        hits = fdr.zdtfdr_protohits_(dest, ws, dev_in, threshold=HIT_SNR, snr=True)
         nh_total += len(hits)
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
@@ -281,7 +280,7 @@ def main():
             "e2e": {"value": e2e_value, "unit": "cells/s",
                     "h2d_bytes_per_step": 4 * NF * NT,
                     "d2h_bytes_per_step": int(16 * nh_total / max(1, e2e_steps)) + 8,
-                    "path": "pinned host spectrogram -> zdtfdr! -> findprotohits(snr=10) -> host"},
+                    "path": "pinned host spectrogram -> zdtfdr! with fused findprotohits(snr=10) -> hits to host"},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None,

@@ -14,7 +14,7 @@ from .arrays import fortran_empty, fortran_zeros, as_device_f32
 from .zdtutils import calcNl, growNr, estimate_memory, driftrates
 from .batchrates import batchrates, RateRange
 from .zdt import (ZDTWorkspace, input_, preprocess_, convolve_, postprocess_, output_,
-                  zdtfdr_, zdtfdr_nodest_, zdtfdr)
+                  zdtfdr_, zdtfdr_nodest_, zdtfdr, zdtfdr_protohits_)
 from .intfdr import intshift, intshift_, intfdr, intfdr_
 from .fftfdr import (FFTFDRWorkspace, fftfdr_workspace, fftfdr_workspace_, fdshiftsum,
                      fdshiftsum_, fdshift, fdshift_, fftfdr, fftfdr_)
@@ -27,7 +27,7 @@ __all__ = [
     "FDRError", "CapacityError", "fortran_empty", "fortran_zeros", "as_device_f32",
     "calcNl", "growNr", "estimate_memory", "driftrates", "batchrates", "RateRange",
     "ZDTWorkspace", "input_", "preprocess_", "convolve_", "postprocess_", "output_",
-    "zdtfdr_", "zdtfdr_nodest_", "zdtfdr",
+    "zdtfdr_", "zdtfdr_nodest_", "zdtfdr", "zdtfdr_protohits_",
     "intshift", "intshift_", "intfdr", "intfdr_",
     "FFTFDRWorkspace", "fftfdr_workspace", "fftfdr_workspace_", "fdshiftsum", "fdshiftsum_",
     "fdshift", "fdshift_", "fftfdr", "fftfdr_",

@@ -109,4 +109,16 @@ void scratch_free(void* p, cudaStream_t s);
 // Current device's SM count (cached per device).
 int sm_count();
 
+// fdrutils.cu helpers shared with the ZDT driver.
+int upload_ptrs(const void* const* host, int64_t nb, void*** dev, cudaStream_t s);
+int stats_device(const float* const* d_mats, int64_t nb, int64_t Nf, int64_t Nrb, double* d_ms,
+                 cudaStream_t s);
+int moments_accumulate(const float* x, long long Nf, long long ncols, double* acc, cudaStream_t s);
+int stats_finalize_launch(const double* acc, long long ncols, long long Nf, double* d_ms,
+                          cudaStream_t s);
+int threshold_launch(const double* d_ms, double snr, double* d_thr, cudaStream_t s);
+int hits_run(const float* const* d_mats, int64_t nb, int64_t Nf, int64_t Nrb, double thr_host,
+             const double* d_thr, int64_t* hits, int64_t capacity, int64_t* count,
+             double* thr_used, cudaStream_t s);
+
 }  // namespace fdr

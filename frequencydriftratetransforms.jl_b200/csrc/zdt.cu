@@ -226,7 +226,7 @@ static int zdt_compute_V(fdr_zdt* ws, cudaStream_t s) {
 }
 
 // One staged ZDT (zdtfdr.jl:355-358) for a given r0 into dest.
-int zdt_staged_run(fdr_zdt* ws, float r0, float* dest, int window, const double* wk,
+int zdt_staged_run(fdr_zdt* ws, float r0, float* dest, int window, const double* wk, double* acc,
                    cudaStream_t s) {
   FDR_TRY(zdt_preprocess(ws, r0, s));
   zdt_mark(ws, "preprocess", s);
@@ -235,6 +235,7 @@ int zdt_staged_run(fdr_zdt* ws, float r0, float* dest, int window, const double*
   FDR_TRY(zdt_postprocess(ws, window, wk, s));
   zdt_mark(ws, "postprocess", s);
   FDR_TRY(zdt_output(ws, dest, s));
+  if (acc) FDR_TRY(moments_accumulate(dest, ws->Nf, ws->Nr, acc, s));
   zdt_mark(ws, "output", s);
   return FDR_OK;
 }
@@ -397,9 +398,9 @@ int fdr_zdt_output(fdr_zdt* ws, float* dest, fdr_stream_t stream) {
   return zdt_output(ws, dest, (cudaStream_t)stream);
 }
 
-int fdr_zdt_execute(fdr_zdt* ws, const float* spectrogram, const float* r0s, int64_t nbatch,
-                    float* const* dests, int window, const double* custom_window,
-                    fdr_stream_t stream) {
+static int zdt_execute(fdr_zdt* ws, const float* spectrogram, const float* r0s, int64_t nbatch,
+                       float* const* dests, int window, const double* custom_window, double* acc,
+                       fdr_stream_t stream) {
   FDR_CHECK_ARG(ws != nullptr, "zdtfdr!: NULL workspace");
   FDR_CHECK_ARG(nbatch >= 0, "zdtfdr!: negative batch count");
   FDR_CHECK_ARG(nbatch == 0 || dests != nullptr, "zdtfdr!: dests is NULL");
@@ -420,9 +421,9 @@ int fdr_zdt_execute(fdr_zdt* ws, const float* spectrogram, const float* r0s, int
   for (int64_t b = 0; b < nbatch; ++b) {
     const float r0 = r0s ? r0s[b] : ws->r0;
     if (use_fused) {
-      FDR_TRY(zdt_fused_run(ws, r0, dests[b], window, custom_window, s));
+      FDR_TRY(zdt_fused_run(ws, r0, dests[b], window, custom_window, acc ? acc + 2 * b * ws->Nr : nullptr, s));
     } else {
-      FDR_TRY(zdt_staged_run(ws, r0, dests[b], window, custom_window, s));
+      FDR_TRY(zdt_staged_run(ws, r0, dests[b], window, custom_window, acc ? acc + 2 * b * ws->Nr : nullptr, s));
     }
   }
   return FDR_OK;
@@ -432,6 +433,41 @@ static void clear_events(fdr_zdt* ws) {
   for (auto e : ws->events) cudaEventDestroy(e);
   ws->events.clear();
   ws->ev_names.clear();
+}
+
+int fdr_zdt_execute(fdr_zdt* ws, const float* spectrogram, const float* r0s, int64_t nbatch,
+                    float* const* dests, int window, const double* custom_window,
+                    fdr_stream_t stream) {
+  return zdt_execute(ws, spectrogram, r0s, nbatch, dests, window, custom_window, nullptr, stream);
+}
+
+int fdr_zdtfdr_protohits(fdr_zdt* ws, const float* spectrogram, const float* r0s, int64_t nbatch,
+                         float* const* dests, int window, const double* custom_window,
+                         double threshold, int snr, int64_t* hits, int64_t capacity,
+                         int64_t* count, double* threshold_used, fdr_stream_t stream) {
+  FDR_CHECK_ARG(ws != nullptr && count != nullptr, "zdtfdr_protohits: NULL argument");
+  FDR_CHECK_ARG(nbatch >= 1, "zdtfdr_protohits: need at least one dest");
+  FDR_CHECK_ARG(capacity >= 0 && (capacity == 0 || hits != nullptr), "zdtfdr_protohits: bad hit buffer");
+  *count = 0;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int64_t ncols = nbatch * ws->Nr;
+  double* acc = nullptr;  // 2*ncols moments, then m, s, threshold
+  if (snr) {
+    FDR_TRY(scratch_alloc((void**)&acc, sizeof(double) * (2 * ncols + 3), s));
+    FDR_CUDA(cudaMemsetAsync(acc, 0, sizeof(double) * 2 * ncols, s));
+  }
+  int st = zdt_execute(ws, spectrogram, r0s, nbatch, dests, window, custom_window, acc, stream);
+  double* d_ms = acc ? acc + 2 * ncols : nullptr;
+  if (st == FDR_OK && snr) st = stats_finalize_launch(acc, ncols, ws->Nf, d_ms, s);
+  if (st == FDR_OK && snr) st = threshold_launch(d_ms, threshold, d_ms + 2, s);
+  void** d_mats = nullptr;
+  if (st == FDR_OK) st = upload_ptrs((const void* const*)dests, nbatch, &d_mats, s);
+  if (st == FDR_OK)
+    st = hits_run((const float* const*)d_mats, nbatch, ws->Nf, ws->Nr, threshold,
+                  snr ? d_ms + 2 : nullptr, hits, capacity, count, threshold_used, s);
+  scratch_free(d_mats, s);
+  scratch_free(acc, s);
+  return st;
 }
 
 int fdr_zdt_set_timing(fdr_zdt* ws, int enable) {

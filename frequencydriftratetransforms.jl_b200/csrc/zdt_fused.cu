@@ -384,7 +384,7 @@ __global__ void __launch_bounds__(Q / 2, 1) zdtf_a2f_kernel(CztArgs a) {
 template <int P, int TC, int T>
 __global__ void __launch_bounds__(T)
 zdtf_output_kernel(const float2* __restrict__ W, long long N, int Q, int Nr, float* __restrict__ dest,
-                   FusedTables tab) {
+                   FusedTables tab, double* __restrict__ acc) {
   constexpr int SS = ac_stride<P, TC>();
   constexpr int TP = TC / 2;
   extern __shared__ float2 sm[];
@@ -418,6 +418,7 @@ zdtf_output_kernel(const float2* __restrict__ W, long long N, int Q, int Nr, flo
   float* d0 = dest + (long long)j * N;
   float* d1 = dest + (long long)(j + 1) * N;
   const bool has1 = (j + 1) < Nr;
+  double m[4] = {0.0, 0.0, 0.0, 0.0};
   for (int e = threadIdx.x; e < TP * P; e += T) {
     const int sp = e % TP, nb = e / TP;
     const long long n = (long long)(na0 + 2 * sp) + (long long)Q * nb;
@@ -425,6 +426,29 @@ zdtf_output_kernel(const float2* __restrict__ W, long long N, int Q, int Nr, flo
     const float2 v1 = buf[(2 * sp + 1) * SS + pidx(nb)];
     __stcs(reinterpret_cast<float2*>(d0 + n), make_float2(v0.x, v1.x));
     if (has1) __stcs(reinterpret_cast<float2*>(d1 + n), make_float2(v0.y, v1.y));
+    if (acc) {
+      m[0] += (double)v0.x + (double)v1.x;
+      m[1] += (double)v0.x * v0.x + (double)v1.x * v1.x;
+      if (has1) {
+        m[2] += (double)v0.y + (double)v1.y;
+        m[3] += (double)v0.y * v0.y + (double)v1.y * v1.y;
+      }
+    }
+  }
+  if (acc) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+      for (int o = 16; o > 0; o >>= 1) m[i] += __shfl_down_sync(0xffffffffu, m[i], o);
+    __shared__ double red[4][T / 32];
+    const int wid = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0)
+      for (int i = 0; i < 4; ++i) red[i][wid] = m[i];
+    __syncthreads();
+    if (threadIdx.x < 4) {
+      double t = 0.0;
+      for (int i = 0; i < T / 32; ++i) t += red[threadIdx.x][i];
+      if (threadIdx.x < 2 || has1) atomicAdd(acc + 2 * j + threadIdx.x, t);
+    }
   }
 }
 
@@ -446,7 +470,8 @@ struct Out2Shape {
 template <int P1, int P2, int TS>
 __global__ void __launch_bounds__(Out2Shape<P1, P2, TS>::T)
 zdtf_output2_kernel(const float2* __restrict__ W, long long N, int Q, int Nr,
-                    float* __restrict__ dest, const float2* __restrict__ rootsP) {
+                    float* __restrict__ dest, const float2* __restrict__ rootsP,
+                    double* __restrict__ acc) {
   using SH = Out2Shape<P1, P2, TS>;
   constexpr int P = SH::P, S1 = SH::S1, SSEQ = SH::SSEQ;
   extern __shared__ float2 sm[];
@@ -472,21 +497,44 @@ zdtf_output2_kernel(const float2* __restrict__ W, long long N, int Q, int Nr,
     }
   }
   __syncthreads();
+  const int j = 2 * q;
+  const bool has1 = (j + 1) < Nr;
+  double m[4] = {0.0, 0.0, 0.0, 0.0};  // sum and sum of squares of the two columns
   if (r < P2) {
     float2 v[P1];
     const float2* b = buf + seq * SSEQ + r;
 #pragma unroll
     for (int k1a = 0; k1a < P1; ++k1a) v[k1a] = b[k1a * S1];
     Dft<P1>::run(v, +1);
-    const int j = 2 * q;
     float* d0 = dest + (long long)j * N + na0 + seq + (long long)Q * r;
     float* d1 = d0 + N;
-    const bool has1 = (j + 1) < Nr;
 #pragma unroll
     for (int nba = 0; nba < P1; ++nba) {
       const long long off = (long long)Q * P2 * nba;
       __stcs(d0 + off, v[nba].x);
       if (has1) __stcs(d1 + off, v[nba].y);
+    }
+    if (acc) {
+#pragma unroll
+      for (int nba = 0; nba < P1; ++nba) {
+        const double x = v[nba].x, y = has1 ? v[nba].y : 0.f;
+        m[0] += x; m[1] += x * x; m[2] += y; m[3] += y * y;
+      }
+    }
+  }
+  if (acc) {  // block reduction of the column moments, then one atomic add per value
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+      for (int o = 16; o > 0; o >>= 1) m[i] += __shfl_down_sync(0xffffffffu, m[i], o);
+    __shared__ double red[4][SH::T / 32];
+    const int wid = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0)
+      for (int i = 0; i < 4; ++i) red[i][wid] = m[i];
+    __syncthreads();
+    if (threadIdx.x < 4) {
+      double t = 0.0;
+      for (int i = 0; i < SH::T / 32; ++i) t += red[threadIdx.x][i];
+      if (threadIdx.x < 2 || has1) atomicAdd(acc + 2 * j + threadIdx.x, t);
     }
   }
 }
@@ -726,16 +774,14 @@ int zdt_fused_A_to_F(fdr_zdt* ws, cudaStream_t s) {
   return FDR_ERR_UNSUPPORTED_SIZE;
 }
 
-int zdt_staged_run(fdr_zdt* ws, float r0, float* dest, int window, const double* wk, cudaStream_t s);
-
 int zdt_fused_run(fdr_zdt* ws, float r0, float* dest, int window, const double* wk,
-                  cudaStream_t s) {
+                  double* acc, cudaStream_t s) {
   FusedState* st = st_of(ws);
   PhaseInt ph;
   if (!ws->A_valid || !make_phase(r0, ws->dr, st->L, &ph)) {
     // No fused input stage to start from (F was set by other means) or rates whose exact
     // phase does not fit 62 bits: run the staged stages.
-    return zdt_staged_run(ws, r0, dest, window, wk, s);
+    return zdt_staged_run(ws, r0, dest, window, wk, acc, s);
   }
   CztArgs a = czt_args(ws, st);
   a.ph = ph;
@@ -768,7 +814,7 @@ int zdt_fused_run(fdr_zdt* ws, float r0, float* dest, int window, const double* 
   if (P == PP) {                                                                               \
     using SH = Out2Shape<P1, P2, 8>;                                                           \
     zdtf_output2_kernel<P1, P2, 8><<<dim3(Q / 8, (unsigned)st->npairs), SH::T, SH::SMEM, s>>>( \
-        ws->W, ws->Nf, Q, (int)ws->Nr, dest, st->tab.rootsP);                                  \
+        ws->W, ws->Nf, Q, (int)ws->Nr, dest, st->tab.rootsP, acc);                             \
     FDR_LAUNCH_CHECK("zdtf_output2_kernel");                                                   \
     zdt_mark(ws, "output", s);                                                                 \
     return FDR_OK;                                                                             \
@@ -783,7 +829,7 @@ int zdt_fused_run(fdr_zdt* ws, float r0, float* dest, int window, const double* 
   if (P == PP) {                                                                               \
     constexpr int TC = AcShape<PP>::TILE, T = AcShape<PP>::T;                                  \
     zdtf_output_kernel<PP, TC, T><<<dim3(Q / TC, (unsigned)st->npairs), T, AcShape<PP>::SMEM, s>>>( \
-        ws->W, ws->Nf, Q, (int)ws->Nr, dest, st->tab);                                         \
+        ws->W, ws->Nf, Q, (int)ws->Nr, dest, st->tab, acc);                                    \
     FDR_LAUNCH_CHECK("zdtf_output_kernel");                                                    \
     zdt_mark(ws, "output", s);                                                                 \
     return FDR_OK;                                                                             \

@@ -46,8 +46,12 @@ bool zdt_fused_eligible(int64_t Nf, int64_t Nt, int64_t Nr);
 int zdt_fused_setup(fdr_zdt* ws);
 int zdt_fused_input(fdr_zdt* ws, const float* spec, cudaStream_t s);
 int zdt_fused_A_to_F(fdr_zdt* ws, cudaStream_t s);
+// acc (may be NULL): per-column float64 sum and sum of squares of dest are added into
+// acc[2*j], acc[2*j+1] while dest is written.
 int zdt_fused_run(fdr_zdt* ws, float r0, float* dest, int window, const double* custom_window,
-                  cudaStream_t s);
+                  double* acc, cudaStream_t s);
+int zdt_staged_run(fdr_zdt* ws, float r0, float* dest, int window, const double* wk, double* acc,
+                   cudaStream_t s);
 void zdt_fused_release(fdr_zdt* ws);
 // timing helpers
 void zdt_mark(fdr_zdt* ws, const char* name, cudaStream_t s);

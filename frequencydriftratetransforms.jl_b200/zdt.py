@@ -256,3 +256,47 @@ def zdtfdr(ws: ZDTWorkspace, spectrogram=None, *, r0=None, w="rect", stream=None
     dest = fortran_empty(ws.Nf, ws.Nr)
     zdtfdr_(dest, ws, spectrogram, r0=r0, w=w, stream=stream)
     return dest
+
+
+def zdtfdr_protohits_(dests, ws: ZDTWorkspace, spectrogram=None, *, r0=None, w="rect",
+                      threshold=10.0, snr=True, capacity=None, stream=None,
+                      return_threshold=False):
+    """zdtfdr!(dests, ws[, spectrogram]; r0) followed by findprotohits(dests, threshold; snr)
+    with the fused threshold/proto-hit scan of the library (fdr_zdtfdr_protohits): the
+    statistics are accumulated while the FDR is written.  Returns an int64 numpy array of
+    zero-based (i, j) hits in column-major order (j offset by b*Nr for the b-th dest)."""
+    single = isinstance(dests, torch.Tensor)
+    dl = [dests] if single else list(dests)
+    for d in dl:
+        _check_dest(ws, d)
+    if r0 is None:
+        r0s = [ws.r0] * len(dl)
+    elif np.ndim(r0) == 0 and not isinstance(r0, (list, tuple)):
+        r0s = [float(np.float32(float(r0)))] * len(dl)
+    else:
+        rl = [float(np.float32(float(x))) for x in r0]
+        r0s = [rl[i % len(rl)] for i in range(len(dl))]
+    spec = None
+    if spectrogram is not None:
+        spec = as_device_f32(spectrogram)
+        _check_spec(ws, spec)
+    code, vals = _window_args(w, ws.K, ws.Nf)
+    n = len(dl)
+    r0_arr = (C.c_float * n)(*r0s)
+    d_arr = (C.c_void_p * n)(*[d.data_ptr() for d in dl])
+    cap = (1 << 20) if capacity is None else int(capacity)
+    hits = torch.empty((max(1, cap), 2), dtype=torch.int64, device="cuda")
+    count, thr = C.c_int64(), C.c_double()
+    st = _lib.lib().fdr_zdtfdr_protohits(ws._h, ptr(spec), r0_arr, n, d_arr, code, ptr(vals),
+                                         float(threshold), 1 if snr else 0, ptr(hits), cap,
+                                         C.byref(count), C.byref(thr), stream_handle(stream))
+    if vals is not None:
+        torch.cuda.current_stream().synchronize()
+    if st == _lib.FDR_ERR_CAPACITY:
+        # the FDR and the threshold are computed: collect the hits with a large enough buffer
+        from .fdrutils import findprotohits
+        out = findprotohits(dl, thr.value, snr=False, capacity=int(count.value), stream=stream)
+        return (out, thr.value) if return_threshold else out
+    _lib.check(st)
+    out = hits[: count.value].cpu().numpy()
+    return (out, thr.value) if return_threshold else out

@@ -138,6 +138,16 @@ int fdr_zdt_output(fdr_zdt* ws, float* dest, fdr_stream_t stream);
 int fdr_zdt_execute(fdr_zdt* ws, const float* spectrogram, const float* r0s, int64_t nbatch,
                     float* const* dests, int window, const double* custom_window,
                     fdr_stream_t stream);
+/* The fused threshold/proto-hit scan: zdtfdr!(dests, ws[, spectrogram]; r0) followed by
+   findprotohits(dests, threshold; snr) (zdtfdr.jl:349-378, fdrutils.jl:148-169).  With snr,
+   the column statistics of fdrstats (fdrutils.jl:39-50) are accumulated while the FDR
+   columns are written, so the FDR is read once more only to count the proto-hits (tiles
+   without hits are not re-read by the write pass).  Hits, count and threshold as in
+   fdr_findprotohits (the batches are the hcat'd matrices).  Synchronises `stream`. */
+int fdr_zdtfdr_protohits(fdr_zdt* ws, const float* spectrogram, const float* r0s, int64_t nbatch,
+                         float* const* dests, int window, const double* custom_window,
+                         double threshold, int snr, int64_t* hits, int64_t capacity,
+                         int64_t* count, double* threshold_used, fdr_stream_t stream);
 /* Per-stage device time of the last fdr_zdt_execute call (enable with
    fdr_zdt_set_timing(ws, 1)); times[i] in milliseconds, names via stage_names. */
 int fdr_zdt_set_timing(fdr_zdt* ws, int enable);

@@ -92,3 +92,24 @@ def test_fused_phase_fallback(fdr, oracle):
     out = fdr.zdtfdr(ws).cpu().numpy()
     truth = oracle.fdr_truth(spec, [1.0, 1.0 + dr, 1.0 + 2 * dr])
     assert oracle.rel_linf(out, truth) < 1e-5
+
+
+@pytest.mark.parametrize("Nf,staged", [(2 ** 16, False), (2 ** 16, True), (2 ** 20, False), (3000, False)])
+def test_fused_protohit_scan(fdr, oracle, Nf, staged):
+    """zdtfdr! + findprotohits with the statistics accumulated by the output kernels."""
+    spec, _ = oracle.synth_spectrogram(Nf, 16, 8, 8.0, 50.0, 4.0, seed=Nf + 3)
+    Nr = 33
+    ws = fdr.ZDTWorkspace(spec, -4.0, 0.25, Nr, staged_only=staged)
+    dests = [fdr.fortran_empty(Nf, Nr) for _ in range(2)]
+    hits, thr = fdr.zdtfdr_protohits_(dests, ws, r0=[-4.0, 4.25], threshold=10.0, snr=True,
+                                      return_threshold=True)
+    mats = [d.cpu().numpy() for d in dests]
+    m, s = oracle.fdrstats(mats)
+    thr_ref = 10.0 * float(np.float32(s)) + float(np.float32(m))
+    assert abs(thr - thr_ref) <= 1e-6 * thr_ref
+    assert np.array_equal(hits, oracle.findprotohits(mats, thr))
+    sep, thr2 = fdr.findprotohits(dests, 10.0, snr=True, return_threshold=True)
+    assert abs(thr2 - thr) <= 1e-6 * thr
+    # absolute threshold (no statistics)
+    hits_abs = fdr.zdtfdr_protohits_(dests, ws, r0=[-4.0, 4.25], threshold=40.0, snr=False)
+    assert np.array_equal(hits_abs, oracle.findprotohits(mats, 40.0))
