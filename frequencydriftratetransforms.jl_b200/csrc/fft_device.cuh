@@ -235,6 +235,60 @@ __device__ __forceinline__ void stockham_pass(float2* buf, const float2* twt) {
   __syncthreads();
 }
 
+// The last pass of an in-place Stockham FFT whose outputs go to emit(seq, i, value)
+// instead of shared memory (natural order i).  Ends with a barrier.
+template <int LEN, int NSEQ, int SSTRIDE, int T, int SIGN, int NS, int R, class Emit>
+__device__ __forceinline__ void stockham_last_pass_emit(float2* buf, const float2* twt, Emit emit) {
+  constexpr int NBF = LEN / R;
+  constexpr int NB = NBF * NSEQ;
+  constexpr int PER = (NB + T - 1) / T;
+  const float2* tw = twt + tw_offset(LEN, NS);
+#pragma unroll
+  for (int i = 0; i < PER; ++i) {
+    const int j = threadIdx.x + i * T;
+    if (NB % T == 0 || j < NB) {
+      const int seq = j / NBF, jj = j - seq * NBF;
+      const int k = jj % NS;
+      float2 v[R];
+      const float2* a = buf + seq * SSTRIDE;
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[r] = a[pidx(jj + r * NBF)];
+      if (NS > 1) {
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          float2 w = tw[(r - 1) * NS + k];
+          if (SIGN > 0) w.y = -w.y;
+          v[r] = cmul(v[r], w);
+        }
+      }
+      Dft<R>::run(v, SIGN);
+      const int base = (jj / NS) * NS * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) emit(seq, base + r * NS, v[r]);
+    }
+  }
+  __syncthreads();
+}
+
+template <int LEN, int NSEQ, int SSTRIDE, int T, int SIGN, int NS, class Emit>
+__device__ __forceinline__ void stockham_passes_emit(float2* buf, const float2* twt, Emit emit) {
+  constexpr int R = plan_radix(LEN / NS);
+  if constexpr (NS * R < LEN) {
+    stockham_pass<LEN, NSEQ, SSTRIDE, T, SIGN, NS, R>(buf, twt);
+    stockham_passes_emit<LEN, NSEQ, SSTRIDE, T, SIGN, NS * R>(buf, twt, emit);
+  } else {
+    stockham_last_pass_emit<LEN, NSEQ, SSTRIDE, T, SIGN, NS, R>(buf, twt, emit);
+  }
+}
+
+// smem_fft whose final pass hands each output to emit(seq, i, value) (no shared store).
+template <int LEN, int NSEQ, int SSTRIDE, int T, int SIGN, class Emit>
+__device__ __forceinline__ void smem_fft_emit(float2* buf, const float2* twt, Emit emit) {
+  static_assert((LEN & (LEN - 1)) == 0, "power-of-two length");
+  static_assert(SSTRIDE >= padlen(LEN), "sequence stride too small");
+  stockham_passes_emit<LEN, NSEQ, SSTRIDE, T, SIGN, 1>(buf, twt, emit);
+}
+
 template <int LEN, int NSEQ, int SSTRIDE, int T, int SIGN, int NS>
 __device__ __forceinline__ void stockham_passes(float2* buf, const float2* twt) {
   if constexpr (NS < LEN) {

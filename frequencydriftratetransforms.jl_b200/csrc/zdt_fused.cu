@@ -334,17 +334,14 @@ __global__ void __launch_bounds__(Q / 2, 1) zdtf_czt_kernel(CztArgs a) {
       }
     }
     __syncthreads();
-    smem_fft<Q, kRatesPerBlock, SS, T, +1>(buf, twt);
-    for (int e = tid; e < kRatesPerBlock * Q / 2; e += T) {
-      const int seq = e / (Q / 2), na = 2 * (e - seq * (Q / 2));
+    // inverse DFT_Q; its last pass writes W (with the inter-pass twiddle and 1/Nf) directly
+    float2* const W = a.W;
+    const int k1a = k1s[0], k1b = k1s[1];
+    smem_fft_emit<Q, kRatesPerBlock, SS, T, +1>(buf, twt, [&](int seq, int na, float2 v) {
       const int q = q0 + (seq >> 1), side = seq & 1;
-      if (q < q_end) {
-        const float2 v0 = cmul(buf[seq * SS + pidx(na)], twr[side * Q + na]);
-        const float2 v1 = cmul(buf[seq * SS + pidx(na + 1)], twr[side * Q + na + 1]);
-        *reinterpret_cast<float4*>(a.W + ((long long)q * P + k1s[side]) * Q + na) =
-            make_float4(v0.x, v0.y, v1.x, v1.y);
-      }
-    }
+      if (q < q_end)
+        W[((long long)q * P + (side ? k1b : k1a)) * Q + na] = cmul(v, twr[side * Q + na]);
+    });
   }
 }
 
