@@ -36,7 +36,8 @@ namespace fdr {
 
 constexpr int kFusedMinLog2 = 12;
 constexpr int kFusedMaxLog2 = 22;
-constexpr int kFusedMaxNt = 16;
+constexpr int kFusedMaxNt = 16;      // F in registers
+constexpr int kFusedMaxNtSmem = 64;  // F in shared memory
 constexpr int kRatesPerBlock = 8;  // 4 rate pairs (8 sequences) per inverse-FFT block in kernel B
 constexpr int kHorner = 4;         // rates evaluated together by one thread (a half block)
 
@@ -345,6 +346,206 @@ __global__ void __launch_bounds__(Q / 2, 1) zdtf_czt_kernel(CztArgs a) {
   }
 }
 
+// ------------------------------------------------------------------------------------
+// Kernel B for 16 < Nt <= NT (32 or 64): F[k, t] of the CTA's Q bases lives in shared
+// memory (t-major, gs[t*Q + base]); T = Q*G threads, G = threads per base, each thread
+// evaluating RPT = 8/G rates of every 8-rate block.  Base b (0 <= b < Q) is side b/(Q/2),
+// k2 = b % (Q/2).
+// ------------------------------------------------------------------------------------
+template <int Q>
+struct CztSmemShape {
+  static constexpr int G = Q >= 512 ? 1 : 2;
+  static constexpr int T = Q * G;
+  static constexpr int RPT = kRatesPerBlock / G;
+  template <int NT>
+  static constexpr size_t smem() {
+    return sizeof(float2) * (kRatesPerBlock * b_stride<Q>() + tw_size(Q) + 2 * Q + NT * Q + NT);
+  }
+};
+
+template <int Q, int NT>
+__device__ __forceinline__ void czt_forward_smem(const CztArgs& a, int c, const int* k1s,
+                                                 float2* buf, const float2* twt, float2* gs,
+                                                 float2* gnyq) {
+  constexpr int T = CztSmemShape<Q>::T;
+  constexpr int SS = b_stride<Q>();
+  constexpr int PC = 4;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < NT * Q; i += T) gs[i] = make_float2(0.f, 0.f);
+  if (c == 0 && tid == 0)
+    for (int t = 0; t < NT; ++t) gnyq[t] = make_float2(0.f, 0.f);
+  for (int p0 = 0; p0 < a.NP; p0 += PC) {
+    __syncthreads();
+    {
+      constexpr int NL = 2 * PC * Q / T;
+      float2 v[NL];
+#pragma unroll
+      for (int i = 0; i < NL; ++i) {
+        const int e = tid + i * T;
+        const int seq = e / Q, na = e - seq * Q;
+        const int pp = p0 + (seq >> 1), side = seq & 1;
+        v[i] = (pp < a.NP) ? __ldcs(a.A + ((long long)pp * a.P + k1s[side]) * Q + na)
+                           : make_float2(0.f, 0.f);
+      }
+#pragma unroll
+      for (int i = 0; i < NL; ++i) {
+        const int e = tid + i * T;
+        const int seq = e / Q, na = e - seq * Q;
+        buf[seq * SS + pidx(na)] = v[i];
+      }
+    }
+    __syncthreads();
+    smem_fft<Q, 2 * PC, SS, T, -1>(buf, twt);
+    for (int e = tid; e < PC * Q; e += T) {
+      const int u = e / Q, b = e - u * Q;
+      if (p0 + u >= a.NP) continue;
+      const int side = b / (Q / 2), k2 = b - side * (Q / 2);
+      int ms, mk2;
+      mirror_of(c, side, k2, Q, &ms, &mk2);
+      const float2 zk = buf[(2 * u + side) * SS + pidx(k2)];
+      const float2 zm = cconj(buf[(2 * u + ms) * SS + pidx(mk2)]);
+      const float2 sm_ = cadd(zk, zm), d = csub(zk, zm);
+      const int t0 = 2 * (p0 + u);
+      gs[t0 * Q + b] = make_float2(0.5f * sm_.x, 0.5f * sm_.y);
+      if (t0 + 1 < NT) gs[(t0 + 1) * Q + b] = make_float2(0.5f * d.y, -0.5f * d.x);
+    }
+    if (c == 0 && tid == 0) {
+      for (int u = 0; u < PC && p0 + u < a.NP; ++u) {
+        const float2 z = buf[(2 * u) * SS + pidx(Q / 2)];
+        const int t0 = 2 * (p0 + u);
+        gnyq[t0] = make_float2(z.x, 0.f);
+        if (t0 + 1 < NT) gnyq[t0 + 1] = make_float2(z.y, 0.f);
+      }
+    }
+  }
+  __syncthreads();
+}
+
+template <int Q, int NT>
+__global__ void __launch_bounds__(CztSmemShape<Q>::T, 1) zdtf_czt_smem_kernel(CztArgs a) {
+  using SH = CztSmemShape<Q>;
+  constexpr int T = SH::T, RPT = SH::RPT;
+  constexpr int SS = b_stride<Q>();
+  extern __shared__ float2 sm[];
+  float2* buf = sm;
+  float2* twt = buf + kRatesPerBlock * SS;
+  float2* twr = twt + tw_size(Q);
+  float2* gs = twr + 2 * Q;
+  float2* gnyq = gs + NT * Q;
+  const int tid = threadIdx.x;
+  const int c = blockIdx.x;
+  const int P = a.P;
+  const int k1s[2] = {c == 0 ? 0 : c, c == 0 ? P / 2 : P - c};
+  const float invN = 1.0f / (float)a.N;
+  for (int i = tid; i < tw_size(Q); i += T) twt[i] = __ldg(a.tab.twQ + i);
+  for (int i = tid; i < 2 * Q; i += T) {
+    const int side = i / Q, na = i - side * Q;
+    twr[i] = cscale(cconj(tw_fwd(a.tab, (long long)k1s[side] * na)), invN);
+  }
+  czt_forward_smem<Q, NT>(a, c, k1s, buf, twt, gs, gnyq);
+
+  const int b = tid % Q, g = tid / Q;
+  const int side = b / (Q / 2), k2 = b - side * (Q / 2);
+  int ms, mk2;
+  mirror_of(c, side, k2, Q, &ms, &mk2);
+  const bool dc = (c == 0 && side == 0 && k2 == 0);
+  const unsigned long long mask = a.ph.mask;
+  const unsigned long long k = (unsigned long long)k1s[side] + (unsigned long long)P * k2;
+  const unsigned long long alpha = (k * a.ph.R0) & mask, beta = (k * a.ph.Rd) & mask;
+  float2 pw[RPT];
+#pragma unroll
+  for (int i = 0; i < RPT; ++i) pw[i] = cis_phase(((unsigned long long)i * beta) & mask, a.ph);
+  const float win = window_value(a, (long long)k);
+  const unsigned long long kny = (unsigned long long)(a.N / 2);
+  const unsigned long long alpha_n = (kny * a.ph.R0) & mask, beta_n = (kny * a.ph.Rd) & mask;
+  const int Nt = a.Nt;
+
+  const int q_begin = blockIdx.y * a.pairs_per_group;
+  const int q_end = min(a.npairs, q_begin + a.pairs_per_group);
+  for (int q0 = q_begin; q0 < q_end; q0 += kRatesPerBlock / 2) {
+    const int j0 = 2 * q0 + g * RPT;  // this thread's first rate of the block
+    const float2 w0 = cis_phase((alpha + (unsigned long long)j0 * beta) & mask, a.ph);
+    float2 w[RPT], S[RPT];
+#pragma unroll
+    for (int jr = 0; jr < RPT; ++jr) {
+      w[jr] = cmul(w0, pw[jr]);
+      S[jr] = gs[(Nt - 1) * Q + b];
+    }
+    for (int t = Nt - 2; t >= 0; --t) {
+      const float2 gt = gs[t * Q + b];
+#pragma unroll
+      for (int jr = 0; jr < RPT; ++jr)
+        S[jr] = make_float2(fmaf(S[jr].x, w[jr].x, fmaf(-S[jr].y, w[jr].y, gt.x)),
+                            fmaf(S[jr].x, w[jr].y, fmaf(S[jr].y, w[jr].x, gt.y)));
+    }
+    __syncthreads();  // buf is free
+#pragma unroll
+    for (int u2 = 0; u2 < RPT / 2; ++u2) {
+      const int u = g * (RPT / 2) + u2;
+      float2 sa = S[2 * u2], sb = S[2 * u2 + 1];
+      sa = (j0 + 2 * u2 < a.Nr) ? cscale(sa, win) : make_float2(0.f, 0.f);
+      sb = (j0 + 2 * u2 + 1 < a.Nr) ? cscale(sb, win) : make_float2(0.f, 0.f);
+      if (dc) {
+        buf[(2 * u) * SS + pidx(0)] = make_float2(sa.x, sb.x);
+      } else {
+        buf[(2 * u + side) * SS + pidx(k2)] = make_float2(sa.x - sb.y, sa.y + sb.x);
+        buf[(2 * u + ms) * SS + pidx(mk2)] = make_float2(sa.x + sb.y, sb.x - sa.y);
+      }
+    }
+    if (c == 0 && tid == 0) {
+      const float wn = window_value(a, (long long)kny);
+      for (int u = 0; u < kRatesPerBlock / 2; ++u) {
+        float v[2];
+        for (int hh = 0; hh < 2; ++hh) {
+          const int j = 2 * q0 + 2 * u + hh;
+          const float2 wv = cis_phase((alpha_n + (unsigned long long)j * beta_n) & mask, a.ph);
+          float2 sv = gnyq[Nt - 1];
+          for (int t = Nt - 2; t >= 0; --t)
+            sv = make_float2(fmaf(sv.x, wv.x, fmaf(-sv.y, wv.y, gnyq[t].x)),
+                             fmaf(sv.x, wv.y, fmaf(sv.y, wv.x, gnyq[t].y)));
+          v[hh] = (j < a.Nr) ? sv.x * wn : 0.f;
+        }
+        buf[(2 * u) * SS + pidx(Q / 2)] = make_float2(v[0], v[1]);
+      }
+    }
+    __syncthreads();
+    float2* const W = a.W;
+    const int k1a = k1s[0], k1b = k1s[1];
+    smem_fft_emit<Q, kRatesPerBlock, SS, T, +1>(buf, twt, [&](int seq, int na, float2 v) {
+      const int q = q0 + (seq >> 1), sd = seq & 1;
+      if (q < q_end)
+        W[((long long)q * P + (sd ? k1b : k1a)) * Q + na] = cmul(v, twr[sd * Q + na]);
+    });
+  }
+}
+
+template <int Q, int NT>
+__global__ void __launch_bounds__(CztSmemShape<Q>::T, 1) zdtf_a2f_smem_kernel(CztArgs a) {
+  using SH = CztSmemShape<Q>;
+  constexpr int T = SH::T;
+  constexpr int SS = b_stride<Q>();
+  extern __shared__ float2 sm[];
+  float2* buf = sm;
+  float2* twt = buf + kRatesPerBlock * SS;
+  float2* twr = twt + tw_size(Q);
+  float2* gs = twr + 2 * Q;
+  float2* gnyq = gs + NT * Q;
+  const int tid = threadIdx.x;
+  const int c = blockIdx.x;
+  const int P = a.P;
+  const int k1s[2] = {c == 0 ? 0 : c, c == 0 ? P / 2 : P - c};
+  for (int i = tid; i < tw_size(Q); i += T) twt[i] = __ldg(a.tab.twQ + i);
+  czt_forward_smem<Q, NT>(a, c, k1s, buf, twt, gs, gnyq);
+  const long long K = a.N / 2 + 1;
+  for (int e = tid; e < Q * a.Nt; e += T) {
+    const int t = e / Q, b = e - t * Q;
+    const int side = b / (Q / 2), k2 = b - side * (Q / 2);
+    a.F[(long long)k1s[side] + (long long)P * k2 + t * K] = gs[t * Q + b];
+  }
+  if (c == 0 && tid == 0)
+    for (int t = 0; t < a.Nt; ++t) a.F[a.N / 2 + t * K] = gnyq[t];
+}
+
 // A -> F (reference layout K x Nt) for the staged stages after a fused input!.
 template <int Q, int NTR>
 __global__ void __launch_bounds__(Q / 2, 1) zdtf_a2f_kernel(CztArgs a) {
@@ -554,10 +755,19 @@ struct CztShape {
       sizeof(float2) * (kRatesPerBlock * b_stride<Q>() + tw_size(Q) + 2 * Q + kFusedMaxNt);
 };
 
+// log2 of the four-step factor Q for Nf = 2^L and Nt time steps: up to 1024 bins per CTA
+// while F fits in registers (Nt <= 16), then 512 (Nt <= 32) and 256 (Nt <= 64) so that
+// F of the CTA's bins fits in shared memory.
+static int fused_qlog(int L, int64_t Nt) {
+  const int cap = Nt <= 16 ? 10 : (Nt <= 32 ? 9 : 8);
+  return std::min(cap, (L + 1) / 2);
+}
+
 bool zdt_fused_eligible(int64_t Nf, int64_t Nt, int64_t Nr) {
-  if (!is_pow2(Nf) || Nt > kFusedMaxNt || Nt < 1 || Nr < 1) return false;
+  if (!is_pow2(Nf) || Nt > kFusedMaxNtSmem || Nt < 1 || Nr < 1) return false;
   const int L = ilog2(Nf);
-  return L >= kFusedMinLog2 && L <= kFusedMaxLog2;
+  if (L < kFusedMinLog2 || L > kFusedMaxLog2) return false;
+  return (L - fused_qlog(L, Nt)) <= 12;  // P <= 4096
 }
 
 static void float_parts(float x, long long* m, int* e) {
@@ -663,6 +873,16 @@ static int set_smem_attrs() {
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CztShape<Q>::SMEM));
   FDR_FOR_Q(SET_B)
 #undef SET_B
+#define SET_BS(Q, NT)                                                                          \
+  FDR_CUDA(cudaFuncSetAttribute(zdtf_czt_smem_kernel<Q, NT>,                                   \
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,                   \
+                                (int)CztSmemShape<Q>::template smem<NT>()));                   \
+  FDR_CUDA(cudaFuncSetAttribute(zdtf_a2f_smem_kernel<Q, NT>,                                   \
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,                   \
+                                (int)CztSmemShape<Q>::template smem<NT>()));
+  SET_BS(64, 32) SET_BS(128, 32) SET_BS(256, 32) SET_BS(512, 32)
+  SET_BS(64, 64) SET_BS(128, 64) SET_BS(256, 64)
+#undef SET_BS
   if (dev < 64) done[dev] = true;
   return FDR_OK;
 }
@@ -671,7 +891,7 @@ static FusedState* st_of(fdr_zdt* ws) { return reinterpret_cast<FusedState*>(ws-
 
 int zdt_fused_setup(fdr_zdt* ws) {
   const int L = ilog2(ws->Nf);
-  const int Qlog = std::min(10, (L + 1) / 2);
+  const int Qlog = fused_qlog(L, ws->Nt);
   ws->fQ = 1 << Qlog;
   ws->fP = (int)(ws->Nf >> Qlog);
   FusedState* st = new FusedState();
@@ -759,6 +979,21 @@ int zdt_fused_A_to_F(fdr_zdt* ws, cudaStream_t s) {
   CztArgs a = czt_args(ws, st);
   a.F = ws->F;
   const int Q = ws->fQ;
+  if (ws->Nt > kFusedMaxNt) {
+    const int NT = ws->Nt <= 32 ? 32 : 64;
+#define LAUNCH_A2FS(QQ, NN)                                                                    \
+    if (Q == QQ && NT == NN) {                                                                 \
+      zdtf_a2f_smem_kernel<QQ, NN><<<ws->fP / 2, CztSmemShape<QQ>::T,                          \
+                                     CztSmemShape<QQ>::template smem<NN>(), s>>>(a);           \
+      FDR_LAUNCH_CHECK("zdtf_a2f_smem_kernel");                                                \
+      return FDR_OK;                                                                           \
+    }
+    LAUNCH_A2FS(64, 32) LAUNCH_A2FS(128, 32) LAUNCH_A2FS(256, 32) LAUNCH_A2FS(512, 32)
+    LAUNCH_A2FS(64, 64) LAUNCH_A2FS(128, 64) LAUNCH_A2FS(256, 64)
+#undef LAUNCH_A2FS
+    set_error(FDR_ERR_UNSUPPORTED_SIZE, "fused A->F: Q=%d Nt=%lld", Q, (long long)ws->Nt);
+    return FDR_ERR_UNSUPPORTED_SIZE;
+  }
 #define LAUNCH_A2F(QQ)                                                                         \
   if (Q == QQ) {                                                                               \
     zdtf_a2f_kernel<QQ, kFusedMaxNt><<<ws->fP / 2, QQ / 2, CztShape<QQ>::SMEM, s>>>(a);        \
@@ -794,13 +1029,28 @@ int zdt_fused_run(fdr_zdt* ws, float r0, float* dest, int window, const double* 
   groups = (int)cdiv(st->npairs, ppg);
   a.pairs_per_group = ppg;
   bool launched = false;
+  if (ws->Nt > kFusedMaxNt) {
+    const int NT = ws->Nt <= 32 ? 32 : 64;
+#define LAUNCH_BS(QQ, NN)                                                                      \
+    if (!launched && Q == QQ && NT == NN) {                                                    \
+      zdtf_czt_smem_kernel<QQ, NN><<<dim3(ctas, groups), CztSmemShape<QQ>::T,                  \
+                                     CztSmemShape<QQ>::template smem<NN>(), s>>>(a);           \
+      FDR_LAUNCH_CHECK("zdtf_czt_smem_kernel");                                                \
+      launched = true;                                                                         \
+    }
+    LAUNCH_BS(64, 32) LAUNCH_BS(128, 32) LAUNCH_BS(256, 32) LAUNCH_BS(512, 32)
+    LAUNCH_BS(64, 64) LAUNCH_BS(128, 64) LAUNCH_BS(256, 64)
+#undef LAUNCH_BS
+  }
 #define LAUNCH_B(QQ)                                                                           \
-  if (Q == QQ) {                                                                               \
+  if (!launched && Q == QQ) {                                                                  \
     zdtf_czt_kernel<QQ, kFusedMaxNt><<<dim3(ctas, groups), QQ / 2, CztShape<QQ>::SMEM, s>>>(a); \
     FDR_LAUNCH_CHECK("zdtf_czt_kernel");                                                       \
     launched = true;                                                                           \
   }
-  FDR_FOR_Q(LAUNCH_B)
+  if (ws->Nt <= kFusedMaxNt) {
+    FDR_FOR_Q(LAUNCH_B)
+  }
 #undef LAUNCH_B
   if (!launched) {
     set_error(FDR_ERR_UNSUPPORTED_SIZE, "fused czt: Q=%d", Q);

@@ -19,7 +19,10 @@ def _spec(oracle, Nf, Nt, seed, ntones=3):
 @pytest.mark.parametrize("Nf,Nt,r0,dr,Nr", [
     (4096, 16, -4.0, 0.25, 33), (4096, 7, 1.5, -0.125, 8), (8192, 16, -2.0, 1 / 16, 5),
     (2 ** 13, 2, 0.0, 0.5, 1), (2 ** 15, 15, -3.0, 0.1, 2), (2 ** 17, 16, -4.0, 0.25, 33),
-    (2 ** 21, 4, -1.0, 0.25, 9), (2 ** 22, 2, 0.5, 1.0, 3)])
+    (2 ** 21, 4, -1.0, 0.25, 9), (2 ** 22, 2, 0.5, 1.0, 3),
+    # F in shared memory (16 < Nt <= 64)
+    (4096, 32, -2.0, 1 / 16, 65), (2 ** 14, 17, -1.0, 0.25, 9), (2 ** 16, 64, -2.0, 1 / 16, 65),
+    (2 ** 18, 33, -8.0, 1 / 16, 257), (2 ** 20, 64, -2.0, 1 / 16, 3)])
 def test_fused_vs_truth_and_staged(fdr, oracle, Nf, Nt, r0, dr, Nr):
     spec = _spec(oracle, Nf, Nt, seed=Nf + Nt)
     ws = fdr.ZDTWorkspace(spec, r0, dr, Nr)
