@@ -54,6 +54,11 @@ class fdr_zdt_info(C.Structure):
     ]
 
 
+class fdr_batch_channel(C.Structure):
+    _fields_ = [("Nf", C.c_int64), ("Nt", C.c_int64), ("Nr", C.c_int64), ("r0", C.c_float),
+                ("dr", C.c_float), ("spectrogram", C.c_void_p), ("fdr", C.c_void_p)]
+
+
 P = C.c_void_p
 I64 = C.c_int64
 F32 = C.c_float
@@ -86,6 +91,13 @@ SIGNATURES = {
     "fdr_zdt_set_timing": (INT, [P, INT]),
     "fdr_zdt_stage_times": (INT, [P, C.POINTER(F32), INT, C.POINTER(INT),
                                   C.POINTER(C.c_char_p)]),
+    "fdr_batch_create": (INT, [C.POINTER(P), C.POINTER(fdr_batch_channel), I64, INT, P]),
+    "fdr_batch_autotune": (INT, [P, P]),
+    "fdr_batch_capture": (INT, [P, P]),
+    "fdr_batch_launch": (INT, [P, P]),
+    "fdr_batch_get_tuning": (INT, [P, C.POINTER(INT), INT, C.POINTER(INT), C.POINTER(INT)]),
+    "fdr_batch_info": (INT, [P, C.POINTER(I64), C.POINTER(I64), C.POINTER(I64), C.POINTER(INT)]),
+    "fdr_batch_destroy": (INT, [P]),
     "fdr_intshift": (INT, [P, I64, I64, F64, INT, P, P]),
     "fdr_intfdr": (INT, [P, I64, I64, C.POINTER(F64), I64, INT, P, P]),
     "fdr_intfdr_shifts": (INT, [P, I64, I64, C.POINTER(I64), I64, P, P]),

@@ -807,9 +807,12 @@ static bool make_phase(float r0, float dr, int L, PhaseInt* ph) {
   return true;
 }
 
-struct FusedState {
-  int L, B;
-  float2* tables = nullptr;  // twP | twQ | tw_lo | tw_hi
+// Sizes and twiddle tables of the fused kernels for one (Nf, Nt, Nr); shared by the ZDT
+// workspace and by batches of channels with the same shape.
+struct FusedPlan {
+  int64_t N = 0, Nt = 0, Nr = 0;
+  int L = 0, B = 0, P = 0, Q = 0;
+  float2* tables = nullptr;  // twP | twQ | tw_lo | tw_hi | rootsP
   FusedTables tab;
   int64_t NP = 0, npairs = 0;
 };
@@ -887,26 +890,29 @@ static int set_smem_attrs() {
   return FDR_OK;
 }
 
-static FusedState* st_of(fdr_zdt* ws) { return reinterpret_cast<FusedState*>(ws->fstate); }
-
-int zdt_fused_setup(fdr_zdt* ws) {
-  const int L = ilog2(ws->Nf);
-  const int Qlog = fused_qlog(L, ws->Nt);
-  ws->fQ = 1 << Qlog;
-  ws->fP = (int)(ws->Nf >> Qlog);
-  FusedState* st = new FusedState();
-  st->L = L;
-  st->B = (L + 1) / 2;
-  st->NP = cdiv(ws->Nt, 2);
-  st->npairs = cdiv(ws->Nr, 2);
-  ws->fstate = st;
-  const long long N = ws->Nf, P = ws->fP, Q = ws->fQ;
+int fused_plan_create(FusedPlan** out, int64_t N, int64_t Nt, int64_t Nr) {
+  *out = nullptr;
+  if (!zdt_fused_eligible(N, Nt, Nr)) {
+    set_error(FDR_ERR_UNSUPPORTED_SIZE, "fused plan: Nf=%lld Nt=%lld not supported",
+              (long long)N, (long long)Nt);
+    return FDR_ERR_UNSUPPORTED_SIZE;
+  }
+  FDR_TRY(set_smem_attrs());
+  FusedPlan* st = new FusedPlan();
+  st->N = N; st->Nt = Nt; st->Nr = Nr;
+  st->L = ilog2(N);
+  const int Qlog = fused_qlog(st->L, Nt);
+  st->Q = 1 << Qlog;
+  st->P = (int)(N >> Qlog);
+  st->B = (st->L + 1) / 2;
+  st->NP = cdiv(Nt, 2);
+  st->npairs = cdiv(Nr, 2);
+  const long long P = st->P, Q = st->Q;
   const long long nlo = 1LL << st->B, nhi = N >> st->B;
   const long long ntwP = tw_size((int)P), ntwQ = tw_size((int)Q);
   const long long ntab = ntwP + ntwQ + nlo + nhi + P;
-  FDR_TRY(set_smem_attrs());
-  cudaError_t e;
-  if ((e = cudaMalloc(&st->tables, sizeof(float2) * ntab)) != cudaSuccess) return cuda_status(e, "cudaMalloc(fused tables)");
+  cudaError_t e = cudaMalloc(&st->tables, sizeof(float2) * ntab);
+  if (e != cudaSuccess) { delete st; return cuda_status(e, "cudaMalloc(fused tables)"); }
   std::vector<float2> h;
   auto append = [&](const std::vector<float2>& v) { h.insert(h.end(), v.begin(), v.end()); };
   append(pass_twiddles((int)P));
@@ -914,42 +920,37 @@ int zdt_fused_setup(fdr_zdt* ws) {
   append(roots_table(1, N, nlo));
   append(roots_table(nlo, N, nhi));
   append(roots_table(1, P, P));
-  if ((e = cudaMemcpy(st->tables, h.data(), sizeof(float2) * ntab, cudaMemcpyHostToDevice)) != cudaSuccess)
-    return cuda_status(e, "upload fused tables");
+  e = cudaMemcpy(st->tables, h.data(), sizeof(float2) * ntab, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) { cudaFree(st->tables); delete st; return cuda_status(e, "upload fused tables"); }
   st->tab.twP = st->tables;
   st->tab.twQ = st->tables + ntwP;
   st->tab.tw_lo = st->tables + ntwP + ntwQ;
   st->tab.tw_hi = st->tables + ntwP + ntwQ + nlo;
   st->tab.rootsP = st->tables + ntwP + ntwQ + nlo + nhi;
   st->tab.B = st->B;
-  if ((e = cudaMalloc(&ws->A, sizeof(float2) * N * st->NP)) != cudaSuccess) return cuda_status(e, "cudaMalloc(A)");
-  ws->W_pairs = st->npairs;
-  if ((e = cudaMalloc(&ws->W, sizeof(float2) * N * ws->W_pairs)) != cudaSuccess) return cuda_status(e, "cudaMalloc(W)");
-  ws->bytes += (int64_t)sizeof(float2) * (ntab + N * st->NP + N * ws->W_pairs);
-  ws->fused = true;
+  *out = st;
   return FDR_OK;
 }
 
-void zdt_fused_release(fdr_zdt* ws) {
-  FusedState* st = st_of(ws);
-  if (st) {
-    cudaFree(st->tables);
-    delete st;
-    ws->fstate = nullptr;
-  }
-  cudaFree(ws->A);
-  cudaFree(ws->W);
-  ws->A = ws->W = nullptr;
+void fused_plan_destroy(FusedPlan* st) {
+  if (!st) return;
+  cudaFree(st->tables);
+  delete st;
 }
 
-int zdt_fused_input(fdr_zdt* ws, const float* spec, cudaStream_t s) {
-  FusedState* st = st_of(ws);
-  const int P = ws->fP, Q = ws->fQ;
+int64_t fused_plan_table_bytes(const FusedPlan* st) {
+  return (int64_t)sizeof(float2) * (tw_size(st->P) + tw_size(st->Q) + (1LL << st->B) + (st->N >> st->B) + st->P);
+}
+int64_t fused_A_elems(const FusedPlan* st) { return st->N * st->NP; }
+int64_t fused_W_elems(const FusedPlan* st) { return st->N * st->npairs; }
+
+int fused_input(const FusedPlan* st, const float* spec, float2* A, cudaStream_t s) {
+  const int P = st->P, Q = st->Q;
 #define LAUNCH_A(PP)                                                                           \
   if (P == PP) {                                                                               \
     constexpr int TA = AcShape<PP>::TILE, T = AcShape<PP>::T;                                  \
     zdtf_input_kernel<PP, TA, T><<<dim3(Q / TA, (unsigned)st->NP), T, AcShape<PP>::SMEM, s>>>( \
-        spec, ws->Nf, (int)ws->Nt, Q, ws->A, st->tab);                                         \
+        spec, st->N, (int)st->Nt, Q, A, st->tab);                                              \
     FDR_LAUNCH_CHECK("zdtf_input_kernel");                                                     \
     return FDR_OK;                                                                             \
   }
@@ -959,31 +960,30 @@ int zdt_fused_input(fdr_zdt* ws, const float* spec, cudaStream_t s) {
   return FDR_ERR_UNSUPPORTED_SIZE;
 }
 
-static CztArgs czt_args(fdr_zdt* ws, FusedState* st) {
+static CztArgs czt_args(const FusedPlan* st, const float2* A, float2* W) {
   CztArgs a;
   memset(&a, 0, sizeof(a));
-  a.A = ws->A;
-  a.W = ws->W;
-  a.N = ws->Nf;
-  a.P = ws->fP;
-  a.Nt = (int)ws->Nt;
+  a.A = A;
+  a.W = W;
+  a.N = st->N;
+  a.P = st->P;
+  a.Nt = (int)st->Nt;
   a.NP = (int)st->NP;
-  a.Nr = (int)ws->Nr;
+  a.Nr = (int)st->Nr;
   a.npairs = (int)st->npairs;
   a.tab = st->tab;
   return a;
 }
 
-int zdt_fused_A_to_F(fdr_zdt* ws, cudaStream_t s) {
-  FusedState* st = st_of(ws);
-  CztArgs a = czt_args(ws, st);
-  a.F = ws->F;
-  const int Q = ws->fQ;
-  if (ws->Nt > kFusedMaxNt) {
-    const int NT = ws->Nt <= 32 ? 32 : 64;
+int fused_a2f(const FusedPlan* st, const float2* A, float2* F, cudaStream_t s) {
+  CztArgs a = czt_args(st, A, nullptr);
+  a.F = F;
+  const int Q = st->Q, ctas = st->P / 2;
+  if (st->Nt > kFusedMaxNt) {
+    const int NT = st->Nt <= 32 ? 32 : 64;
 #define LAUNCH_A2FS(QQ, NN)                                                                    \
     if (Q == QQ && NT == NN) {                                                                 \
-      zdtf_a2f_smem_kernel<QQ, NN><<<ws->fP / 2, CztSmemShape<QQ>::T,                          \
+      zdtf_a2f_smem_kernel<QQ, NN><<<ctas, CztSmemShape<QQ>::T,                                \
                                      CztSmemShape<QQ>::template smem<NN>(), s>>>(a);           \
       FDR_LAUNCH_CHECK("zdtf_a2f_smem_kernel");                                                \
       return FDR_OK;                                                                           \
@@ -991,12 +991,12 @@ int zdt_fused_A_to_F(fdr_zdt* ws, cudaStream_t s) {
     LAUNCH_A2FS(64, 32) LAUNCH_A2FS(128, 32) LAUNCH_A2FS(256, 32) LAUNCH_A2FS(512, 32)
     LAUNCH_A2FS(64, 64) LAUNCH_A2FS(128, 64) LAUNCH_A2FS(256, 64)
 #undef LAUNCH_A2FS
-    set_error(FDR_ERR_UNSUPPORTED_SIZE, "fused A->F: Q=%d Nt=%lld", Q, (long long)ws->Nt);
+    set_error(FDR_ERR_UNSUPPORTED_SIZE, "fused A->F: Q=%d Nt=%lld", Q, (long long)st->Nt);
     return FDR_ERR_UNSUPPORTED_SIZE;
   }
 #define LAUNCH_A2F(QQ)                                                                         \
   if (Q == QQ) {                                                                               \
-    zdtf_a2f_kernel<QQ, kFusedMaxNt><<<ws->fP / 2, QQ / 2, CztShape<QQ>::SMEM, s>>>(a);        \
+    zdtf_a2f_kernel<QQ, kFusedMaxNt><<<ctas, QQ / 2, CztShape<QQ>::SMEM, s>>>(a);              \
     FDR_LAUNCH_CHECK("zdtf_a2f_kernel");                                                       \
     return FDR_OK;                                                                             \
   }
@@ -1006,64 +1006,69 @@ int zdt_fused_A_to_F(fdr_zdt* ws, cudaStream_t s) {
   return FDR_ERR_UNSUPPORTED_SIZE;
 }
 
-int zdt_fused_run(fdr_zdt* ws, float r0, float* dest, int window, const double* wk,
-                  double* acc, cudaStream_t s) {
-  FusedState* st = st_of(ws);
+bool fused_phase_ok(const FusedPlan* st, float r0, float dr) {
   PhaseInt ph;
-  if (!ws->A_valid || !make_phase(r0, ws->dr, st->L, &ph)) {
-    // No fused input stage to start from (F was set by other means) or rates whose exact
-    // phase does not fit 62 bits: run the staged stages.
-    return zdt_staged_run(ws, r0, dest, window, wk, acc, s);
+  return make_phase(r0, dr, st->L, &ph);
+}
+
+// Rate groups (grid.y of the czt kernel) by default: about four waves of one CTA per SM.
+int fused_default_groups(const FusedPlan* st) {
+  const int ctas = st->P / 2;
+  return std::max(1, std::min<int>((int)cdiv(4 * sm_count(), ctas),
+                                   (int)cdiv(st->npairs, kRatesPerBlock / 2)));
+}
+
+int fused_czt(const FusedPlan* st, const float2* A, float2* W, float r0, float dr, int window,
+              const double* wk, int groups, cudaStream_t s) {
+  PhaseInt ph;
+  if (!make_phase(r0, dr, st->L, &ph)) {
+    set_error(FDR_ERR_UNSUPPORTED_SIZE, "fused czt: rates need more than 62 phase bits");
+    return FDR_ERR_UNSUPPORTED_SIZE;
   }
-  CztArgs a = czt_args(ws, st);
+  CztArgs a = czt_args(st, A, W);
   a.ph = ph;
   a.window = window;
   a.wk = wk;
-  const int P = ws->fP, Q = ws->fQ;
-  // rate groups: enough CTAs for about four waves of one CTA per SM
-  const int ctas = P / 2;
-  int groups = std::max(1, std::min<int>((int)cdiv(4 * sm_count(), ctas),
-                                         (int)cdiv(st->npairs, kRatesPerBlock / 2)));
+  const int Q = st->Q, ctas = st->P / 2;
+  if (groups <= 0) groups = fused_default_groups(st);
   int ppg = (int)cdiv(st->npairs, groups);
   ppg = (int)cdiv(ppg, kRatesPerBlock / 2) * (kRatesPerBlock / 2);
   groups = (int)cdiv(st->npairs, ppg);
   a.pairs_per_group = ppg;
-  bool launched = false;
-  if (ws->Nt > kFusedMaxNt) {
-    const int NT = ws->Nt <= 32 ? 32 : 64;
+  if (st->Nt > kFusedMaxNt) {
+    const int NT = st->Nt <= 32 ? 32 : 64;
 #define LAUNCH_BS(QQ, NN)                                                                      \
-    if (!launched && Q == QQ && NT == NN) {                                                    \
+    if (Q == QQ && NT == NN) {                                                                 \
       zdtf_czt_smem_kernel<QQ, NN><<<dim3(ctas, groups), CztSmemShape<QQ>::T,                  \
                                      CztSmemShape<QQ>::template smem<NN>(), s>>>(a);           \
       FDR_LAUNCH_CHECK("zdtf_czt_smem_kernel");                                                \
-      launched = true;                                                                         \
+      return FDR_OK;                                                                           \
     }
     LAUNCH_BS(64, 32) LAUNCH_BS(128, 32) LAUNCH_BS(256, 32) LAUNCH_BS(512, 32)
     LAUNCH_BS(64, 64) LAUNCH_BS(128, 64) LAUNCH_BS(256, 64)
 #undef LAUNCH_BS
-  }
+  } else {
 #define LAUNCH_B(QQ)                                                                           \
-  if (!launched && Q == QQ) {                                                                  \
-    zdtf_czt_kernel<QQ, kFusedMaxNt><<<dim3(ctas, groups), QQ / 2, CztShape<QQ>::SMEM, s>>>(a); \
-    FDR_LAUNCH_CHECK("zdtf_czt_kernel");                                                       \
-    launched = true;                                                                           \
-  }
-  if (ws->Nt <= kFusedMaxNt) {
+    if (Q == QQ) {                                                                             \
+      zdtf_czt_kernel<QQ, kFusedMaxNt><<<dim3(ctas, groups), QQ / 2, CztShape<QQ>::SMEM, s>>>(a); \
+      FDR_LAUNCH_CHECK("zdtf_czt_kernel");                                                     \
+      return FDR_OK;                                                                           \
+    }
     FDR_FOR_Q(LAUNCH_B)
-  }
 #undef LAUNCH_B
-  if (!launched) {
-    set_error(FDR_ERR_UNSUPPORTED_SIZE, "fused czt: Q=%d", Q);
-    return FDR_ERR_UNSUPPORTED_SIZE;
   }
-  zdt_mark(ws, "czt", s);
+  set_error(FDR_ERR_UNSUPPORTED_SIZE, "fused czt: Q=%d Nt=%lld", Q, (long long)st->Nt);
+  return FDR_ERR_UNSUPPORTED_SIZE;
+}
+
+int fused_output(const FusedPlan* st, const float2* W, float* dest, double* acc, cudaStream_t s) {
+  const int P = st->P, Q = st->Q;
 #define LAUNCH_C2(PP, P1, P2)                                                                  \
   if (P == PP) {                                                                               \
     using SH = Out2Shape<P1, P2, 8>;                                                           \
     zdtf_output2_kernel<P1, P2, 8><<<dim3(Q / 8, (unsigned)st->npairs), SH::T, SH::SMEM, s>>>( \
-        ws->W, ws->Nf, Q, (int)ws->Nr, dest, st->tab.rootsP, acc);                             \
+        W, st->N, Q, (int)st->Nr, dest, st->tab.rootsP, acc);                                  \
     FDR_LAUNCH_CHECK("zdtf_output2_kernel");                                                   \
-    zdt_mark(ws, "output", s);                                                                 \
     return FDR_OK;                                                                             \
   }
   LAUNCH_C2(64, 8, 8)
@@ -1076,15 +1081,61 @@ int zdt_fused_run(fdr_zdt* ws, float r0, float* dest, int window, const double* 
   if (P == PP) {                                                                               \
     constexpr int TC = AcShape<PP>::TILE, T = AcShape<PP>::T;                                  \
     zdtf_output_kernel<PP, TC, T><<<dim3(Q / TC, (unsigned)st->npairs), T, AcShape<PP>::SMEM, s>>>( \
-        ws->W, ws->Nf, Q, (int)ws->Nr, dest, st->tab, acc);                                    \
+        W, st->N, Q, (int)st->Nr, dest, st->tab, acc);                                         \
     FDR_LAUNCH_CHECK("zdtf_output_kernel");                                                    \
-    zdt_mark(ws, "output", s);                                                                 \
     return FDR_OK;                                                                             \
   }
   FDR_FOR_P(LAUNCH_C)
 #undef LAUNCH_C
   set_error(FDR_ERR_UNSUPPORTED_SIZE, "fused output: P=%d", P);
   return FDR_ERR_UNSUPPORTED_SIZE;
+}
+
+// ---- workspace wrappers ----------------------------------------------------------------
+static FusedPlan* st_of(fdr_zdt* ws) { return reinterpret_cast<FusedPlan*>(ws->fstate); }
+
+int zdt_fused_setup(fdr_zdt* ws) {
+  FusedPlan* st = nullptr;
+  FDR_TRY(fused_plan_create(&st, ws->Nf, ws->Nt, ws->Nr));
+  ws->fstate = st;
+  ws->fP = st->P;
+  ws->fQ = st->Q;
+  cudaError_t e;
+  if ((e = cudaMalloc(&ws->A, sizeof(float2) * fused_A_elems(st))) != cudaSuccess) return cuda_status(e, "cudaMalloc(A)");
+  ws->W_pairs = st->npairs;
+  if ((e = cudaMalloc(&ws->W, sizeof(float2) * fused_W_elems(st))) != cudaSuccess) return cuda_status(e, "cudaMalloc(W)");
+  ws->bytes += fused_plan_table_bytes(st) + (int64_t)sizeof(float2) * (fused_A_elems(st) + fused_W_elems(st));
+  ws->fused = true;
+  return FDR_OK;
+}
+
+void zdt_fused_release(fdr_zdt* ws) {
+  fused_plan_destroy(st_of(ws));
+  ws->fstate = nullptr;
+  cudaFree(ws->A);
+  cudaFree(ws->W);
+  ws->A = ws->W = nullptr;
+}
+
+int zdt_fused_input(fdr_zdt* ws, const float* spec, cudaStream_t s) {
+  return fused_input(st_of(ws), spec, ws->A, s);
+}
+
+int zdt_fused_A_to_F(fdr_zdt* ws, cudaStream_t s) { return fused_a2f(st_of(ws), ws->A, ws->F, s); }
+
+int zdt_fused_run(fdr_zdt* ws, float r0, float* dest, int window, const double* wk,
+                  double* acc, cudaStream_t s) {
+  FusedPlan* st = st_of(ws);
+  if (!ws->A_valid || !fused_phase_ok(st, r0, ws->dr)) {
+    // No fused input stage to start from (F was set by other means) or rates whose exact
+    // phase does not fit 62 bits: run the staged stages.
+    return zdt_staged_run(ws, r0, dest, window, wk, acc, s);
+  }
+  FDR_TRY(fused_czt(st, ws->A, ws->W, r0, ws->dr, window, wk, 0, s));
+  zdt_mark(ws, "czt", s);
+  FDR_TRY(fused_output(st, ws->W, dest, acc, s));
+  zdt_mark(ws, "output", s);
+  return FDR_OK;
 }
 
 }  // namespace fdr

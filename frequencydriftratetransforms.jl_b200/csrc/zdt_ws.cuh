@@ -53,6 +53,21 @@ int zdt_fused_run(fdr_zdt* ws, float r0, float* dest, int window, const double* 
 int zdt_staged_run(fdr_zdt* ws, float r0, float* dest, int window, const double* wk, double* acc,
                    cudaStream_t s);
 void zdt_fused_release(fdr_zdt* ws);
+
+// Fused kernels for one (Nf, Nt, Nr) shape with caller-owned intermediates (zdt_fused.cu).
+struct FusedPlan;
+int fused_plan_create(FusedPlan** out, int64_t N, int64_t Nt, int64_t Nr);
+void fused_plan_destroy(FusedPlan* st);
+int64_t fused_plan_table_bytes(const FusedPlan* st);
+int64_t fused_A_elems(const FusedPlan* st);
+int64_t fused_W_elems(const FusedPlan* st);
+bool fused_phase_ok(const FusedPlan* st, float r0, float dr);
+int fused_default_groups(const FusedPlan* st);
+int fused_input(const FusedPlan* st, const float* spec, float2* A, cudaStream_t s);
+int fused_a2f(const FusedPlan* st, const float2* A, float2* F, cudaStream_t s);
+int fused_czt(const FusedPlan* st, const float2* A, float2* W, float r0, float dr, int window,
+              const double* wk, int groups, cudaStream_t s);
+int fused_output(const FusedPlan* st, const float2* W, float* dest, double* acc, cudaStream_t s);
 // timing helpers
 void zdt_mark(fdr_zdt* ws, const char* name, cudaStream_t s);
 }  // namespace fdr

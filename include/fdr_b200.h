@@ -155,6 +155,37 @@ int fdr_zdt_stage_times(fdr_zdt* ws, float* times_ms, int max_stages, int* nstag
                         const char** stage_names);
 
 /* ---------------------------------------------------------------------------------- */
+/* Batches of coarse channels (no single reference function: the reference runs one      */
+/* zdtfdr! per spectrogram; pipelines loop over coarse channels, README.md:57-71)          */
+/* ---------------------------------------------------------------------------------- */
+typedef struct fdr_batch fdr_batch;
+typedef struct fdr_batch_channel {
+  int64_t Nf, Nt, Nr;        /* spectrogram Nf x Nt; rates r0 + j*dr, j < Nr */
+  float r0, dr;
+  const float* spectrogram;  /* device, Nf x Nt column-major */
+  float* fdr;                /* device, Nf x Nr column-major (written by each launch) */
+} fdr_batch_channel;
+/* Plan nch channels of any shapes over `slots` streams (1..16): channels of equal
+   (Nf, Nt, Nr) share one fused plan; each slot owns intermediates sized for the largest
+   channel.  The channel array (host) is copied; the device arrays must outlive the batch. */
+int fdr_batch_create(fdr_batch** batch, const fdr_batch_channel* channels, int64_t nch,
+                     int slots, fdr_stream_t stream);
+/* Autotuner: per distinct shape, the czt kernel's rate-group split (timed over 1, 2, 4, 8),
+   then the number of active slots (timed over powers of two up to `slots`); cached per shape
+   for the process.  Call before fdr_batch_capture.  Synchronises `stream`. */
+int fdr_batch_autotune(fdr_batch* batch, fdr_stream_t stream);
+/* Records the whole batch (forked over the active slot streams) into one CUDA graph;
+   `stream` must not be the legacy default stream.  Runs the batch once eagerly first. */
+int fdr_batch_capture(fdr_batch* batch, fdr_stream_t stream);
+/* Computes every channel's FDR: one cudaGraphLaunch when captured, else eager launches. */
+int fdr_batch_launch(fdr_batch* batch, fdr_stream_t stream);
+int fdr_batch_get_tuning(const fdr_batch* batch, int* groups, int ngroups, int* nplans,
+                         int* active_slots);
+int fdr_batch_info(const fdr_batch* batch, int64_t* nchannels, int64_t* nfused, int64_t* bytes,
+                   int* captured);
+int fdr_batch_destroy(fdr_batch* batch);
+
+/* ---------------------------------------------------------------------------------- */
 /* intfdr.jl                                                                           */
 /* ---------------------------------------------------------------------------------- */
 /* intshift! (intfdr.jl:7-14): dout[:, t] = circshift(din[:, t], -round(rate*t)). */
