@@ -16,6 +16,7 @@ from .batchrates import batchrates, RateRange
 from .zdt import (ZDTWorkspace, input_, preprocess_, convolve_, postprocess_, output_,
                   zdtfdr_, zdtfdr_nodest_, zdtfdr, zdtfdr_protohits_)
 from .batch import ZDTBatch
+from . import proposal
 from .intfdr import intshift, intshift_, intfdr, intfdr_
 from .fftfdr import (FFTFDRWorkspace, fftfdr_workspace, fftfdr_workspace_, fdshiftsum,
                      fdshiftsum_, fdshift, fdshift_, fftfdr, fftfdr_)
@@ -28,7 +29,7 @@ __all__ = [
     "FDRError", "CapacityError", "fortran_empty", "fortran_zeros", "as_device_f32",
     "calcNl", "growNr", "estimate_memory", "driftrates", "batchrates", "RateRange",
     "ZDTWorkspace", "input_", "preprocess_", "convolve_", "postprocess_", "output_",
-    "zdtfdr_", "zdtfdr_nodest_", "zdtfdr", "zdtfdr_protohits_", "ZDTBatch",
+    "zdtfdr_", "zdtfdr_nodest_", "zdtfdr", "zdtfdr_protohits_", "ZDTBatch", "proposal",
     "intshift", "intshift_", "intfdr", "intfdr_",
     "FFTFDRWorkspace", "fftfdr_workspace", "fftfdr_workspace_", "fdshiftsum", "fdshiftsum_",
     "fdshift", "fdshift_", "fftfdr", "fftfdr_",

@@ -98,6 +98,16 @@ SIGNATURES = {
     "fdr_batch_get_tuning": (INT, [P, C.POINTER(INT), INT, C.POINTER(INT), C.POINTER(INT)]),
     "fdr_batch_info": (INT, [P, C.POINTER(I64), C.POINTER(I64), C.POINTER(I64), C.POINTER(INT)]),
     "fdr_batch_destroy": (INT, [P]),
+    "fdr_propose_create": (INT, [C.POINTER(P), INT, INT, INT, INT, INT, INT, C.c_uint64]),
+    "fdr_propose_destroy": (INT, [P]),
+    "fdr_propose_num_params": (INT, [P, C.POINTER(I64)]),
+    "fdr_propose_features": (INT, [P, I64, I64, INT, P, P]),
+    "fdr_propose_lag_features": (INT, [P, I64, I64, INT, INT, P, P]),
+    "fdr_propose_forward": (INT, [P, P, INT, P, P]),
+    "fdr_propose_gradients": (INT, [P, P, P, INT, P, P, P, P]),
+    "fdr_propose_train_step": (INT, [P, P, P, INT, F32, P, P, P]),
+    "fdr_propose_get_state": (INT, [P, P, P, P, C.POINTER(I64)]),
+    "fdr_propose_set_state": (INT, [P, P, P, P, I64]),
     "fdr_intshift": (INT, [P, I64, I64, F64, INT, P, P]),
     "fdr_intfdr": (INT, [P, I64, I64, C.POINTER(F64), I64, INT, P, P]),
     "fdr_intfdr_shifts": (INT, [P, I64, I64, C.POINTER(I64), I64, P, P]),

@@ -262,7 +262,7 @@ __global__ void __launch_bounds__(Q / 2, 1) zdtf_czt_kernel(CztArgs a) {
   // kHorner at a time, w = w(first rate of the group, exact) * pw[jr] (exact).
   const unsigned long long mask = a.ph.mask;
   unsigned long long alpha[2], beta[2];
-  float2 pw[2][kHorner];
+  float2 pw[2][kHorner + 1];  // exact w(k, i*dr) for i < kHorner, and for i = kHorner
   float win[2];
 #pragma unroll
   for (int b = 0; b < 2; ++b) {
@@ -270,7 +270,7 @@ __global__ void __launch_bounds__(Q / 2, 1) zdtf_czt_kernel(CztArgs a) {
     alpha[b] = (k * a.ph.R0) & mask;
     beta[b] = (k * a.ph.Rd) & mask;
 #pragma unroll
-    for (int i = 0; i < kHorner; ++i) pw[b][i] = cis_phase(((unsigned long long)i * beta[b]) & mask, a.ph);
+    for (int i = 0; i <= kHorner; ++i) pw[b][i] = cis_phase(((unsigned long long)i * beta[b]) & mask, a.ph);
     win[b] = window_value(a, (long long)k);
   }
   // Nyquist bin (CTA 0, thread 0)
@@ -287,13 +287,17 @@ __global__ void __launch_bounds__(Q / 2, 1) zdtf_czt_kernel(CztArgs a) {
   for (int q0 = q_begin; q0 < q_end; q0 += kRatesPerBlock / 2) {
     const int j0 = 2 * q0;
     __syncthreads();  // buf is free
+    // exact phase of the block's first rate; the second half starts at w0 * w(k, 4*dr)
+    float2 wb[2];
+#pragma unroll
+    for (int b = 0; b < 2; ++b) wb[b] = cis_phase((alpha[b] + (unsigned long long)j0 * beta[b]) & mask, a.ph);
 #pragma unroll
     for (int h = 0; h < kRatesPerBlock / kHorner; ++h) {
       const int jh = j0 + h * kHorner;
       float2 S[2][kHorner];
 #pragma unroll
       for (int b = 0; b < 2; ++b) {
-        const float2 w0 = cis_phase((alpha[b] + (unsigned long long)jh * beta[b]) & mask, a.ph);
+        const float2 w0 = (h == 0) ? wb[b] : cmul(wb[b], pw[b][kHorner]);
 #pragma unroll
         for (int jr = 0; jr < kHorner; ++jr) {
           const float2 w = cmul(w0, pw[b][jr]);

@@ -186,6 +186,45 @@ int fdr_batch_info(const fdr_batch* batch, int64_t* nchannels, int64_t* nfused, 
 int fdr_batch_destroy(fdr_batch* batch);
 
 /* ---------------------------------------------------------------------------------- */
+/* Learned drift-rate window proposal (no reference counterpart: a training/serving     */
+/* extension of the batched rate search, batchrates.jl:22-60, zdtfdr.jl:354)             */
+/* ---------------------------------------------------------------------------------- */
+typedef struct fdr_propose_net fdr_propose_net;
+/* 4-layer 1-D conv net over nbins coarse bins with nt input channels (nt <= 64): three k=5 layers of
+   `width` channels with ReLU, a 1x1 layer to nwin window logits, max over bins.  This build
+   supports width 32, ksize 5, nwin 16.  Weights: seeded He-uniform, float32 master copy,
+   float16 copy used by the forward pass.  max_batch bounds the batch of every call. */
+int fdr_propose_create(fdr_propose_net** net, int nbins, int nt, int width, int ksize, int nwin,
+                       int max_batch, uint64_t seed);
+int fdr_propose_destroy(fdr_propose_net* net);
+int fdr_propose_num_params(const fdr_propose_net* net, int64_t* count);
+/* Network input of one spectrogram (Nf x Nt): out[t][bin] = (sum of `factor` consecutive
+   channels - factor) / sqrt(factor), bin < Nf/factor (device, Nt x Nf/factor row-major). */
+int fdr_propose_features(const float* spectrogram, int64_t Nf, int64_t Nt, int factor,
+                         float* out, fdr_stream_t stream);
+/* Drift evidence of one spectrogram: out[l + maxlag][bin] = sum over the `factor` channels n
+   of the bin and over t < Nt-1 of (s[n,t] - 1) * (s[(n + l) mod Nf, t+1] - 1), divided by
+   sqrt(factor * (Nt - 1)), for lags l in [-maxlag, maxlag] (maxlag 8, factor <= 4096; device,
+   (2*maxlag+1) x Nf/factor row-major).  Zero mean, unit variance for an exponential(1)
+   background; a tone drifting r channels per step shows up at lags floor(r) and ceil(r). */
+int fdr_propose_lag_features(const float* spectrogram, int64_t Nf, int64_t Nt, int factor,
+                             int maxlag, float* out, fdr_stream_t stream);
+/* logits[b][w] (device) for x[b][t][bin] (device), b < batch. */
+int fdr_propose_forward(fdr_propose_net* net, const float* x, int batch, float* logits,
+                        fdr_stream_t stream);
+/* Mean binary cross-entropy with labels[b][w] in {0,1}; gradient of every parameter into
+   grad_out (device, num_params floats; may be NULL) and the loss into loss_out (device). */
+int fdr_propose_gradients(fdr_propose_net* net, const float* x, const float* labels, int batch,
+                          float* logits, float* grad_out, float* loss_out, fdr_stream_t stream);
+/* One Adam step (beta 0.9/0.999, eps 1e-8) at learning rate lr; deterministic. */
+int fdr_propose_train_step(fdr_propose_net* net, const float* x, const float* labels, int batch,
+                           float lr, float* logits, float* loss_out, fdr_stream_t stream);
+/* Checkpoint state (HOST arrays of num_params floats): weights, Adam moments, step count. */
+int fdr_propose_get_state(fdr_propose_net* net, float* params, float* m, float* v, int64_t* step);
+int fdr_propose_set_state(fdr_propose_net* net, const float* params, const float* m, const float* v,
+                          int64_t step);
+
+/* ---------------------------------------------------------------------------------- */
 /* intfdr.jl                                                                           */
 /* ---------------------------------------------------------------------------------- */
 /* intshift! (intfdr.jl:7-14): dout[:, t] = circshift(din[:, t], -round(rate*t)). */

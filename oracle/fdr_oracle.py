@@ -550,3 +550,100 @@ def rel_l2(a, b):
     a = np.asarray(a, dtype=np.float64)
     b = np.asarray(b, dtype=np.float64)
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+# ----------------------------------------------------------------------------------------
+# FP64 restatement of the proposal network (gradient check of its CUDA kernels)
+# ----------------------------------------------------------------------------------------
+
+def propose_layers(nt, width=32, ksize=5, nwin=16):
+    """(cin, cout, k) of the four convolution layers, in parameter order (w then b)."""
+    return [(nt, width, ksize), (width, width, ksize), (width, width, ksize), (width, nwin, 1)]
+
+
+def propose_unpack(params, nt, width=32, ksize=5, nwin=16):
+    out, off = [], 0
+    for cin, cout, k in propose_layers(nt, width, ksize, nwin):
+        w = params[off:off + cout * cin * k].reshape(cout, cin, k)
+        off += cout * cin * k
+        b = params[off:off + cout]
+        off += cout
+        out.append((w, b))
+    return out
+
+
+def propose_loss_and_grad(params, x, labels, nt, half_weights=True):
+    """Mean BCE-with-logits of the net on x (B, nt, X) and its gradient wrt params, in
+    float64 (weights rounded to float16 first, as the forward pass of the kernels uses)."""
+    p = np.asarray(params, np.float64)
+    layers = propose_unpack(p, nt)
+    if half_weights:
+        layers = [(w.astype(np.float16).astype(np.float64), b) for w, b in layers]
+    x = np.asarray(x, np.float64)
+    B, _, X = x.shape
+    acts = [x]
+    for li, (w, b) in enumerate(layers):
+        cout, cin, k = w.shape
+        pad = k // 2
+        xin = np.pad(acts[-1], ((0, 0), (0, 0), (pad, pad)))
+        y = np.zeros((B, cout, X))
+        for kk in range(k):
+            y += np.einsum("oc,bcx->box", w[:, :, kk], xin[:, :, kk:kk + X])
+        y += b[None, :, None]
+        if li < 3:
+            y = np.maximum(y, 0.0)
+        acts.append(y)
+    y4 = acts[-1]
+    am = np.argmax(y4, axis=2)
+    z = np.take_along_axis(y4, am[:, :, None], axis=2)[:, :, 0]
+    lab = np.asarray(labels, np.float64)
+    n = z.size
+    loss = np.mean(np.maximum(z, 0) - z * lab + np.log1p(np.exp(-np.abs(z))))
+    dz = (1.0 / (1.0 + np.exp(-z)) - lab) / n
+    dy = np.zeros_like(y4)
+    np.put_along_axis(dy, am[:, :, None], dz[:, :, None], axis=2)
+    grads = []
+    for li in range(3, -1, -1):
+        w, b = layers[li]
+        cout, cin, k = w.shape
+        pad = k // 2
+        if li < 3:
+            dy = dy * (acts[li + 1] > 0)
+        xin = np.pad(acts[li], ((0, 0), (0, 0), (pad, pad)))
+        gw = np.zeros_like(w)
+        for kk in range(k):
+            gw[:, :, kk] = np.einsum("box,bcx->oc", dy, xin[:, :, kk:kk + X])
+        gb = dy.sum(axis=(0, 2))
+        grads.append((gw, gb))
+        if li > 0:
+            dpad = np.pad(dy, ((0, 0), (0, 0), (pad, pad)))
+            din = np.zeros_like(acts[li])
+            for kk in range(k):
+                # d in[x] += w[k] * dy[x - k + pad]
+                din += np.einsum("oc,box->bcx", w[:, :, kk], dpad[:, :, (k - 1 - kk):(k - 1 - kk) + X])
+            dy = din
+    flat = []
+    for gw, gb in reversed(grads):
+        flat.append(gw.ravel())
+        flat.append(gb)
+    return loss, np.concatenate(flat)
+
+
+def propose_features(spec, factor=256):
+    """Power input of the proposal net: (Nt, Nf/factor), (group sum - factor)/sqrt(factor)."""
+    s = np.asarray(spec, np.float64)
+    Nf, Nt = s.shape
+    g = s.reshape(Nf // factor, factor, Nt).sum(axis=1)
+    return ((g - factor) / math.sqrt(factor)).T
+
+
+def propose_lag_features(spec, factor=256, maxlag=8):
+    """Drift evidence input: (2*maxlag+1, Nf/factor); row l+maxlag = per-bin sums over
+    t < Nt-1 of (s[n,t]-1)(s[(n+l) mod Nf,t+1]-1), divided by sqrt(factor*(Nt-1))."""
+    s = np.asarray(spec, np.float64) - 1.0
+    Nf, Nt = s.shape
+    out = np.empty((2 * maxlag + 1, Nf // factor))
+    for li, l in enumerate(range(-maxlag, maxlag + 1)):
+        prod = (s[:, :-1] * np.roll(s[:, 1:], -l, axis=0)).sum(axis=1)
+        out[li] = prod.reshape(Nf // factor, factor).sum(axis=1)
+    return out / math.sqrt(factor * (Nt - 1))

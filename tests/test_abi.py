@@ -71,3 +71,23 @@ def test_rate_range_params(fdr):
     rr = fdr.batchrates(16, 1.0, -4.0)[0]
     assert rr.first == rr.start and len(rr) == rr.length
     assert list(rr)[1] - list(rr)[0] == rr.step
+
+
+def test_proposal_calibration_host_logic(fdr):
+    """Threshold calibration of the proposal search (host code, no GPU)."""
+    import numpy as np
+    P = fdr.proposal
+    rng = np.random.default_rng(0)
+    counts = np.zeros((50, 16), np.int64)
+    probs = np.full((50, 16), 0.001)
+    for i in range(50):
+        w = rng.choice(16, 2, replace=False)
+        counts[i, w] = rng.integers(1, 20, 2)
+        probs[i, w] = rng.uniform(0.3, 0.99, 2)
+    cal = P.calibrate(probs, counts, target=1.0)
+    assert cal["window_recall"] == 1.0 and cal["fallback_rate"] == 0.0
+    assert cal["cost"] == 100.0  # exactly the two positive windows per channel
+    # hide one positive window below every other probability: recall 1.0 needs fallback
+    probs[0, np.nonzero(counts[0])[0][0]] = 0.0005
+    cal = P.calibrate(probs, counts, target=1.0)
+    assert cal["window_recall"] == 1.0 and cal["cost"] > 100.0

@@ -125,3 +125,38 @@ def test_batchrates_properties(oracle):
         span = {round(lo / dh), round(hi / dh)}
         covered = {int(r * (Nt - 1)) for r in flat}
         assert span <= covered
+
+
+def test_proposal_restatement_finite_differences(oracle):
+    """The FP64 restatement of the proposal net (the checker of the CUDA gradients) agrees
+    with central finite differences of its own loss."""
+    rng = np.random.default_rng(0)
+    nt, X, B = 3, 20, 2
+    n = sum(co * ci * k + co for ci, co, k in oracle.propose_layers(nt))
+    p = rng.normal(0, 0.3, n)
+    x = rng.normal(0, 1, (B, nt, X))
+    lab = (rng.random((B, 16)) < 0.3).astype(float)
+    _, g = oracle.propose_loss_and_grad(p, x, lab, nt, half_weights=False)
+    eps = 1e-6
+    for i in rng.choice(n, 24, replace=False):
+        q = p.copy()
+        q[i] += eps
+        l1, _ = oracle.propose_loss_and_grad(q, x, lab, nt, half_weights=False)
+        q[i] -= 2 * eps
+        l2, _ = oracle.propose_loss_and_grad(q, x, lab, nt, half_weights=False)
+        fd = (l1 - l2) / (2 * eps)
+        assert abs(fd - g[i]) <= 1e-5 * max(abs(fd), 1e-3)
+
+
+def test_proposal_features_restatement(oracle):
+    rng = np.random.default_rng(1)
+    Nf, Nt = 1024, 4
+    s = -np.log(rng.random((Nf, Nt)))
+    p = oracle.propose_features(s, factor=256)
+    assert p.shape == (Nt, 4)
+    assert np.allclose(p[2, 1], (s[256:512, 2].sum() - 256) / 16)
+    lf = oracle.propose_lag_features(s, factor=256, maxlag=8)
+    l, b = 3, 2  # lag +3 of bin 2, with wrap-around inside the sum
+    ref = sum((s[n, t] - 1) * (s[(n + l) % Nf, t + 1] - 1)
+              for n in range(512, 768) for t in range(Nt - 1)) / np.sqrt(256 * (Nt - 1))
+    assert np.isclose(lf[l + 8, b], ref)
