@@ -14,7 +14,8 @@ from .arrays import fortran_empty, fortran_zeros, as_device_f32
 from .zdtutils import calcNl, growNr, estimate_memory, driftrates
 from .batchrates import batchrates, RateRange
 from .zdt import (ZDTWorkspace, input_, preprocess_, convolve_, postprocess_, output_,
-                  zdtfdr_, zdtfdr_nodest_, zdtfdr, zdtfdr_protohits_)
+                  zdtfdr_, zdtfdr_nodest_, zdtfdr, zdtfdr_protohits_, zdtfdr_blocks_,
+                  zdtfdr_blocks_protohits_)
 from .batch import ZDTBatch
 from . import proposal
 from .intfdr import intshift, intshift_, intfdr, intfdr_
@@ -29,7 +30,8 @@ __all__ = [
     "FDRError", "CapacityError", "fortran_empty", "fortran_zeros", "as_device_f32",
     "calcNl", "growNr", "estimate_memory", "driftrates", "batchrates", "RateRange",
     "ZDTWorkspace", "input_", "preprocess_", "convolve_", "postprocess_", "output_",
-    "zdtfdr_", "zdtfdr_nodest_", "zdtfdr", "zdtfdr_protohits_", "ZDTBatch", "proposal",
+    "zdtfdr_", "zdtfdr_nodest_", "zdtfdr", "zdtfdr_protohits_", "zdtfdr_blocks_",
+    "zdtfdr_blocks_protohits_", "ZDTBatch", "proposal",
     "intshift", "intshift_", "intfdr", "intfdr_",
     "FFTFDRWorkspace", "fftfdr_workspace", "fftfdr_workspace_", "fdshiftsum", "fdshiftsum_",
     "fdshift", "fdshift_", "fftfdr", "fftfdr_",

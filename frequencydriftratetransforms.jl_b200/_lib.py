@@ -88,6 +88,9 @@ SIGNATURES = {
     "fdr_zdt_execute": (INT, [P, P, C.POINTER(F32), I64, C.POINTER(P), INT, P, P]),
     "fdr_zdtfdr_protohits": (INT, [P, P, C.POINTER(F32), I64, C.POINTER(P), INT, P, F64, INT, P,
                                    I64, C.POINTER(I64), C.POINTER(F64), P]),
+    "fdr_zdt_execute_blocks": (INT, [P, P, C.POINTER(C.c_int32), I64, P, INT, P, P]),
+    "fdr_zdtfdr_blocks_protohits": (INT, [P, P, C.POINTER(C.c_int32), I64, P, INT, P, F64, INT, P,
+                                          I64, C.POINTER(I64), C.POINTER(F64), P]),
     "fdr_zdt_set_timing": (INT, [P, INT]),
     "fdr_zdt_stage_times": (INT, [P, C.POINTER(F32), INT, C.POINTER(INT),
                                   C.POINTER(C.c_char_p)]),

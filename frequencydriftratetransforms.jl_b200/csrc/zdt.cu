@@ -429,6 +429,41 @@ static int zdt_execute(fdr_zdt* ws, const float* spectrogram, const float* r0s, 
   return FDR_OK;
 }
 
+// zdtfdr! over 8-rate blocks of the workspace's rate grid in one pass (fused path only).
+static int zdt_execute_blocks(fdr_zdt* ws, const float* spectrogram, const int32_t* blocks,
+                              int64_t nblocks, float* dest, int window, const double* custom_window,
+                              double* acc, cudaStream_t s) {
+  FDR_CHECK_ARG(ws != nullptr && blocks != nullptr && dest != nullptr, "zdtfdr blocks: NULL argument");
+  FDR_CHECK_ARG(nblocks >= 1, "zdtfdr blocks: need at least one block");
+  if (window < 0 || window > 2) {
+    set_error(FDR_ERR_UNSUPPORTED_WINDOW, "unsupported window type (%d)", window);
+    return FDR_ERR_UNSUPPORTED_WINDOW;
+  }
+  FDR_CHECK_ARG(window != FDR_WINDOW_CUSTOM || custom_window != nullptr,
+                "zdtfdr blocks: custom window values are NULL");
+  if (!ws->fused || (ws->flags & FDR_ZDT_STAGED_ONLY)) {
+    set_error(FDR_ERR_UNSUPPORTED_SIZE, "zdtfdr blocks: needs the fused path (power-of-two Nf, Nt <= 64)");
+    return FDR_ERR_UNSUPPORTED_SIZE;
+  }
+  for (int64_t i = 0; i < nblocks; ++i)
+    FDR_CHECK_ARG(blocks[i] >= 0 && 8LL * (blocks[i] + 1) <= ws->Nr,
+                  "zdtfdr blocks: block %lld = %d outside the workspace's %lld rates", (long long)i,
+                  (int)blocks[i], (long long)ws->Nr);
+  FDR_CHECK_ARG(4 * nblocks <= ws->W_pairs, "zdtfdr blocks: more than Nr/8 blocks");
+  int* d_blk = nullptr;
+  FDR_TRY(scratch_alloc((void**)&d_blk, sizeof(int) * nblocks, s));
+  int st = cuda_status(cudaMemcpyAsync(d_blk, blocks, sizeof(int) * nblocks, cudaMemcpyHostToDevice, s),
+                       "upload rate blocks");
+  zdt_mark(ws, "start", s);
+  if (st == FDR_OK && spectrogram) {
+    st = fdr_zdt_input(ws, spectrogram, s);
+    zdt_mark(ws, "input", s);
+  }
+  if (st == FDR_OK) st = zdt_fused_run_blocks(ws, d_blk, nblocks, dest, window, custom_window, acc, s);
+  scratch_free(d_blk, s);
+  return st;
+}
+
 static void clear_events(fdr_zdt* ws) {
   for (auto e : ws->events) cudaEventDestroy(e);
   ws->events.clear();
@@ -464,6 +499,43 @@ int fdr_zdtfdr_protohits(fdr_zdt* ws, const float* spectrogram, const float* r0s
   if (st == FDR_OK) st = upload_ptrs((const void* const*)dests, nbatch, &d_mats, s);
   if (st == FDR_OK)
     st = hits_run((const float* const*)d_mats, nbatch, ws->Nf, ws->Nr, threshold,
+                  snr ? d_ms + 2 : nullptr, hits, capacity, count, threshold_used, s);
+  scratch_free(d_mats, s);
+  scratch_free(acc, s);
+  return st;
+}
+
+int fdr_zdt_execute_blocks(fdr_zdt* ws, const float* spectrogram, const int32_t* blocks,
+                           int64_t nblocks, float* dest, int window, const double* custom_window,
+                           fdr_stream_t stream) {
+  return zdt_execute_blocks(ws, spectrogram, blocks, nblocks, dest, window, custom_window, nullptr,
+                            (cudaStream_t)stream);
+}
+
+int fdr_zdtfdr_blocks_protohits(fdr_zdt* ws, const float* spectrogram, const int32_t* blocks,
+                                int64_t nblocks, float* dest, int window, const double* custom_window,
+                                double threshold, int snr, int64_t* hits, int64_t capacity,
+                                int64_t* count, double* threshold_used, fdr_stream_t stream) {
+  FDR_CHECK_ARG(ws != nullptr && count != nullptr, "zdtfdr_blocks_protohits: NULL argument");
+  FDR_CHECK_ARG(nblocks >= 1, "zdtfdr_blocks_protohits: need at least one block");
+  FDR_CHECK_ARG(capacity >= 0 && (capacity == 0 || hits != nullptr), "zdtfdr_blocks_protohits: bad hit buffer");
+  *count = 0;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int64_t ncols = 8 * nblocks;
+  double* acc = nullptr;  // 2*ncols moments, then m, s, threshold
+  if (snr) {
+    FDR_TRY(scratch_alloc((void**)&acc, sizeof(double) * (2 * ncols + 3), s));
+    FDR_CUDA(cudaMemsetAsync(acc, 0, sizeof(double) * 2 * ncols, s));
+  }
+  int st = zdt_execute_blocks(ws, spectrogram, blocks, nblocks, dest, window, custom_window, acc, s);
+  double* d_ms = acc ? acc + 2 * ncols : nullptr;
+  if (st == FDR_OK && snr) st = stats_finalize_launch(acc, ncols, ws->Nf, d_ms, s);
+  if (st == FDR_OK && snr) st = threshold_launch(d_ms, threshold, d_ms + 2, s);
+  void** d_mats = nullptr;
+  float* const dl[1] = {dest};
+  if (st == FDR_OK) st = upload_ptrs((const void* const*)dl, 1, &d_mats, s);
+  if (st == FDR_OK)
+    st = hits_run((const float* const*)d_mats, 1, ws->Nf, ncols, threshold,
                   snr ? d_ms + 2 : nullptr, hits, capacity, count, threshold_used, s);
   scratch_free(d_mats, s);
   scratch_free(acc, s);

@@ -132,6 +132,8 @@ struct CztArgs {
   float2* W;          // [pair][k1][na] for pairs [0, npairs)
   float2* F;          // A->F mode output (K x Nt) or NULL
   const double* wk;   // custom window values (K) or NULL
+  const int* blk_base;  // rate index (on the r0 + j*dr grid) of each 8-rate block's first
+                        // rate, or NULL for 8*block (the contiguous rates 0..Nr-1)
   long long N;
   int P, Nt, NP, Nr, npairs, pairs_per_group, window;
   PhaseInt ph;
@@ -286,11 +288,12 @@ __global__ void __launch_bounds__(Q / 2, 1) zdtf_czt_kernel(CztArgs a) {
   const int q_end = min(a.npairs, q_begin + a.pairs_per_group);
   for (int q0 = q_begin; q0 < q_end; q0 += kRatesPerBlock / 2) {
     const int j0 = 2 * q0;
+    const long long jg = a.blk_base ? (long long)__ldg(a.blk_base + (q0 >> 2)) : (long long)j0;
     __syncthreads();  // buf is free
     // exact phase of the block's first rate; the second half starts at w0 * w(k, 4*dr)
     float2 wb[2];
 #pragma unroll
-    for (int b = 0; b < 2; ++b) wb[b] = cis_phase((alpha[b] + (unsigned long long)j0 * beta[b]) & mask, a.ph);
+    for (int b = 0; b < 2; ++b) wb[b] = cis_phase((alpha[b] + (unsigned long long)jg * beta[b]) & mask, a.ph);
 #pragma unroll
     for (int h = 0; h < kRatesPerBlock / kHorner; ++h) {
       const int jh = j0 + h * kHorner;
@@ -331,7 +334,7 @@ __global__ void __launch_bounds__(Q / 2, 1) zdtf_czt_kernel(CztArgs a) {
 #pragma unroll
         for (int hh = 0; hh < 2; ++hh) {
           const int j = j0 + 2 * u + hh;
-          const float2 w = cis_phase((alpha_n + (unsigned long long)j * beta_n) & mask, a.ph);
+          const float2 w = cis_phase((alpha_n + (unsigned long long)(jg + 2 * u + hh) * beta_n) & mask, a.ph);
           const float2 sv = horner<NTR>(Gn, w);
           v[hh] = (j < a.Nr) ? sv.x * wn : 0.f;  // real-only Nyquist bin
         }
@@ -468,7 +471,8 @@ __global__ void __launch_bounds__(CztSmemShape<Q>::T, 1) zdtf_czt_smem_kernel(Cz
   const int q_end = min(a.npairs, q_begin + a.pairs_per_group);
   for (int q0 = q_begin; q0 < q_end; q0 += kRatesPerBlock / 2) {
     const int j0 = 2 * q0 + g * RPT;  // this thread's first rate of the block
-    const float2 w0 = cis_phase((alpha + (unsigned long long)j0 * beta) & mask, a.ph);
+    const long long jb = a.blk_base ? (long long)__ldg(a.blk_base + (q0 >> 2)) : (long long)(2 * q0);
+    const float2 w0 = cis_phase((alpha + (unsigned long long)(jb + g * RPT) * beta) & mask, a.ph);
     float2 w[RPT], S[RPT];
 #pragma unroll
     for (int jr = 0; jr < RPT; ++jr) {
@@ -502,7 +506,7 @@ __global__ void __launch_bounds__(CztSmemShape<Q>::T, 1) zdtf_czt_smem_kernel(Cz
         float v[2];
         for (int hh = 0; hh < 2; ++hh) {
           const int j = 2 * q0 + 2 * u + hh;
-          const float2 wv = cis_phase((alpha_n + (unsigned long long)j * beta_n) & mask, a.ph);
+          const float2 wv = cis_phase((alpha_n + (unsigned long long)(jb + 2 * u + hh) * beta_n) & mask, a.ph);
           float2 sv = gnyq[Nt - 1];
           for (int t = Nt - 2; t >= 0; --t)
             sv = make_float2(fmaf(sv.x, wv.x, fmaf(-sv.y, wv.y, gnyq[t].x)),
@@ -1024,6 +1028,12 @@ int fused_default_groups(const FusedPlan* st) {
 
 int fused_czt(const FusedPlan* st, const float2* A, float2* W, float r0, float dr, int window,
               const double* wk, int groups, cudaStream_t s) {
+  return fused_czt_blocks(st, A, W, r0, dr, window, wk, nullptr, groups, s);
+}
+
+int fused_czt_blocks(const FusedPlan* st, const float2* A, float2* W, float r0, float dr,
+                     int window, const double* wk, const int* blk_base, int groups,
+                     cudaStream_t s) {
   PhaseInt ph;
   if (!make_phase(r0, dr, st->L, &ph)) {
     set_error(FDR_ERR_UNSUPPORTED_SIZE, "fused czt: rates need more than 62 phase bits");
@@ -1033,6 +1043,7 @@ int fused_czt(const FusedPlan* st, const float2* A, float2* W, float r0, float d
   a.ph = ph;
   a.window = window;
   a.wk = wk;
+  a.blk_base = blk_base;
   const int Q = st->Q, ctas = st->P / 2;
   if (groups <= 0) groups = fused_default_groups(st);
   int ppg = (int)cdiv(st->npairs, groups);
@@ -1138,6 +1149,27 @@ int zdt_fused_run(fdr_zdt* ws, float r0, float* dest, int window, const double* 
   FDR_TRY(fused_czt(st, ws->A, ws->W, r0, ws->dr, window, wk, 0, s));
   zdt_mark(ws, "czt", s);
   FDR_TRY(fused_output(st, ws->W, dest, acc, s));
+  zdt_mark(ws, "output", s);
+  return FDR_OK;
+}
+
+// A subset of the workspace's rates: nblocks blocks of 8 consecutive rates, block i starting
+// at rate index blk_base[i] (device) of the r0 + j*dr grid; the FDR columns 8i..8i+7 of dest.
+// The plan's tables are shared; only the rate count differs.
+int zdt_fused_run_blocks(fdr_zdt* ws, const int* blk_base, int64_t nblocks, float* dest,
+                         int window, const double* wk, double* acc, cudaStream_t s) {
+  const FusedPlan* st = st_of(ws);
+  FDR_CHECK_ARG(ws->A_valid, "zdtfdr blocks: the workspace holds no fused input stage");
+  FDR_CHECK_ARG(fused_phase_ok(st, ws->r0, ws->dr), "zdtfdr blocks: rates need more than 62 phase bits");
+  FDR_CHECK_ARG(nblocks >= 1 && 4 * nblocks <= ws->W_pairs,
+                "zdtfdr blocks: %lld blocks exceed the workspace's %lld rates", (long long)nblocks,
+                (long long)(2 * ws->W_pairs));
+  FusedPlan sub = *st;
+  sub.Nr = 8 * nblocks;
+  sub.npairs = 4 * nblocks;
+  FDR_TRY(fused_czt_blocks(&sub, ws->A, ws->W, ws->r0, ws->dr, window, wk, blk_base, 0, s));
+  zdt_mark(ws, "czt", s);
+  FDR_TRY(fused_output(&sub, ws->W, dest, acc, s));
   zdt_mark(ws, "output", s);
   return FDR_OK;
 }

@@ -67,7 +67,12 @@ int fused_input(const FusedPlan* st, const float* spec, float2* A, cudaStream_t 
 int fused_a2f(const FusedPlan* st, const float2* A, float2* F, cudaStream_t s);
 int fused_czt(const FusedPlan* st, const float2* A, float2* W, float r0, float dr, int window,
               const double* wk, int groups, cudaStream_t s);
+int fused_czt_blocks(const FusedPlan* st, const float2* A, float2* W, float r0, float dr,
+                     int window, const double* wk, const int* blk_base, int groups,
+                     cudaStream_t s);
 int fused_output(const FusedPlan* st, const float2* W, float* dest, double* acc, cudaStream_t s);
+int zdt_fused_run_blocks(fdr_zdt* ws, const int* blk_base, int64_t nblocks, float* dest,
+                         int window, const double* wk, double* acc, cudaStream_t s);
 // timing helpers
 void zdt_mark(fdr_zdt* ws, const char* name, cudaStream_t s);
 }  // namespace fdr

@@ -33,7 +33,7 @@ import torch
 
 from . import _lib
 from .arrays import fortran_empty, ptr, stream_handle
-from .zdt import ZDTWorkspace, zdtfdr_protohits_
+from .zdt import ZDTWorkspace, zdtfdr_blocks_protohits_, zdtfdr_protohits_
 
 NWIN, RATES_PER_WIN = 16, 16
 DR = 1.0 / 16
@@ -278,10 +278,10 @@ class ProposalSearch:
     Per channel, with p_w the window probabilities: windows with p_w >= tau_hi are run; a
     window with tau <= p_w < tau_hi is uncertain, and a channel with any uncertain window
     (or with more than ``max_windows`` windows to run) falls back to the full 256-rate
-    search.  The proposed windows run as rate batches of one 16-rate workspace through the
-    r0 iterator (one input stage per channel); the proto-hit threshold is denormalised
-    from the statistics of the windows that ran (findprotohits over an iterable of FDR
-    matrices, fdrutils.jl:156-169)."""
+    search.  The proposed windows run in one pass of the fused kernels over their 8-rate
+    blocks (zdtfdr_blocks_protohits_, sharing the full search's workspace); the proto-hit
+    threshold is denormalised from the statistics of the columns that ran (findprotohits
+    over an iterable of FDR matrices, fdrutils.jl:156-169)."""
 
     def __init__(self, net, tau=0.05, tau_hi=None, max_windows=NWIN, Nf=1 << 20, Nt=16,
                  full=None):
@@ -290,8 +290,6 @@ class ProposalSearch:
         self.tau_hi = tau if tau_hi is None else tau_hi
         self.max_windows = max_windows
         self.Nf, self.Nt = Nf, Nt
-        self.win_ws = ZDTWorkspace(None, R_MIN, DR, RATES_PER_WIN, shape=(Nf, Nt))
-        self.win_dests = [fortran_empty(Nf, RATES_PER_WIN) for _ in range(NWIN)]
         self.full = full or FullSearch(Nf, Nt)
 
     def decide(self, p):
@@ -318,12 +316,13 @@ class ProposalSearch:
             return self.full.hits(spec, snr), NRATES, True
         if len(wins) == 0:
             return np.zeros((0, 2), np.int64), 0, False
-        dests = [self.win_dests[w] for w in wins]
-        h = zdtfdr_protohits_(dests, self.win_ws, spec, r0=[R_MIN + float(w) for w in wins],
-                              threshold=snr, snr=True)
+        per = RATES_PER_WIN // 8
+        blocks = (wins[:, None] * per + np.arange(per)[None, :]).ravel()
+        dest = self.full.dest[:, :8 * len(blocks)]
+        h = zdtfdr_blocks_protohits_(dest, self.full.ws, spec, blocks, threshold=snr, snr=True)
         if len(h):
             h = h.copy()
-            h[:, 1] = wins[h[:, 1] // RATES_PER_WIN] * RATES_PER_WIN + h[:, 1] % RATES_PER_WIN
+            h[:, 1] = blocks[h[:, 1] // 8] * 8 + h[:, 1] % 8
         return h, len(wins) * RATES_PER_WIN, False
 
 

@@ -300,3 +300,61 @@ def zdtfdr_protohits_(dests, ws: ZDTWorkspace, spectrogram=None, *, r0=None, w="
     _lib.check(st)
     out = hits[: count.value].cpu().numpy()
     return (out, thr.value) if return_threshold else out
+
+
+def _blocks_args(ws, dest, blocks):
+    bl = [int(b) for b in np.asarray(blocks).ravel()]
+    if not bl:
+        raise _lib.FDRError(_lib.FDR_ERR_INVALID_ARGUMENT, "need at least one rate block")
+    from .arrays import is_fortran
+    if (not isinstance(dest, torch.Tensor) or dest.dtype != torch.float32
+            or dest.device.type != "cuda" or tuple(dest.shape) != (ws.Nf, 8 * len(bl))
+            or not is_fortran(dest)):
+        raise _lib.FDRError(_lib.FDR_ERR_INVALID_ARGUMENT,
+                            f"dest must be a column-major float32 CUDA ({ws.Nf}, {8 * len(bl)}) matrix")
+    return (C.c_int32 * len(bl))(*bl), len(bl)
+
+
+def zdtfdr_blocks_(dest, ws: ZDTWorkspace, spectrogram, blocks, *, w="rect", stream=None):
+    """zdtfdr! over the 8-rate blocks ``blocks`` of the workspace's rate grid in one pass
+    (fdr_zdt_execute_blocks): FDR column 8i+u of ``dest`` is rate r0 + (8*blocks[i]+u)*dr."""
+    barr, nb = _blocks_args(ws, dest, blocks)
+    spec = None
+    if spectrogram is not None:
+        spec = as_device_f32(spectrogram)
+        _check_spec(ws, spec)
+    code, vals = _window_args(w, ws.K, ws.Nf)
+    _lib.check(_lib.lib().fdr_zdt_execute_blocks(ws._h, ptr(spec), barr, nb, ptr(dest), code,
+                                                 ptr(vals), stream_handle(stream)))
+    if vals is not None:
+        torch.cuda.current_stream().synchronize()
+    return dest
+
+
+def zdtfdr_blocks_protohits_(dest, ws: ZDTWorkspace, spectrogram, blocks, *, w="rect",
+                             threshold=10.0, snr=True, capacity=None, stream=None,
+                             return_threshold=False):
+    """zdtfdr_blocks_ followed by the fused proto-hit scan of ``dest``
+    (fdr_zdtfdr_blocks_protohits); hits are zero-based (i, dest column) pairs."""
+    barr, nb = _blocks_args(ws, dest, blocks)
+    spec = None
+    if spectrogram is not None:
+        spec = as_device_f32(spectrogram)
+        _check_spec(ws, spec)
+    code, vals = _window_args(w, ws.K, ws.Nf)
+    cap = (1 << 20) if capacity is None else int(capacity)
+    hits = torch.empty((max(1, cap), 2), dtype=torch.int64, device="cuda")
+    count, thr = C.c_int64(), C.c_double()
+    st = _lib.lib().fdr_zdtfdr_blocks_protohits(ws._h, ptr(spec), barr, nb, ptr(dest), code,
+                                                ptr(vals), float(threshold), 1 if snr else 0,
+                                                ptr(hits), cap, C.byref(count), C.byref(thr),
+                                                stream_handle(stream))
+    if vals is not None:
+        torch.cuda.current_stream().synchronize()
+    if st == _lib.FDR_ERR_CAPACITY:
+        from .fdrutils import findprotohits
+        out = findprotohits(dest, thr.value, snr=False, capacity=int(count.value), stream=stream)
+        return (out, thr.value) if return_threshold else out
+    _lib.check(st)
+    out = hits[: count.value].cpu().numpy()
+    return (out, thr.value) if return_threshold else out

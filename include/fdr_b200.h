@@ -148,6 +148,22 @@ int fdr_zdtfdr_protohits(fdr_zdt* ws, const float* spectrogram, const float* r0s
                          float* const* dests, int window, const double* custom_window,
                          double threshold, int snr, int64_t* hits, int64_t capacity,
                          int64_t* count, double* threshold_used, fdr_stream_t stream);
+/* zdtfdr! over a subset of the workspace's drift rates in one pass: nblocks blocks of 8
+   consecutive rates, block i covering rates r0 + (8*blocks[i] + u)*dr (u < 8, host array,
+   8*(blocks[i]+1) <= Nr, 8*nblocks <= Nr rounded up to even), written to the FDR columns
+   8i..8i+7 of dest (device, Nf x 8*nblocks column-major).  One input stage and one pass of
+   the fused kernels for all blocks, so a sparse set of rate windows costs in proportion to
+   its size (the r0 iterator of zdtfdr!, zdtfdr.jl:354, pays a full pass per r0).  No
+   counterpart in the reference; fused workspaces only (FDR_ERR_UNSUPPORTED_SIZE else). */
+int fdr_zdt_execute_blocks(fdr_zdt* ws, const float* spectrogram, const int32_t* blocks,
+                           int64_t nblocks, float* dest, int window, const double* custom_window,
+                           fdr_stream_t stream);
+/* fdr_zdt_execute_blocks followed by the fused threshold/proto-hit scan of its dest, as
+   fdr_zdtfdr_protohits (statistics over the computed columns; hit j is the dest column). */
+int fdr_zdtfdr_blocks_protohits(fdr_zdt* ws, const float* spectrogram, const int32_t* blocks,
+                                int64_t nblocks, float* dest, int window, const double* custom_window,
+                                double threshold, int snr, int64_t* hits, int64_t capacity,
+                                int64_t* count, double* threshold_used, fdr_stream_t stream);
 /* Per-stage device time of the last fdr_zdt_execute call (enable with
    fdr_zdt_set_timing(ws, 1)); times[i] in milliseconds, names via stage_names. */
 int fdr_zdt_set_timing(fdr_zdt* ws, int enable);

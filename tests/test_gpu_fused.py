@@ -116,3 +116,40 @@ def test_fused_protohit_scan(fdr, oracle, Nf, staged):
     # absolute threshold (no statistics)
     hits_abs = fdr.zdtfdr_protohits_(dests, ws, r0=[-4.0, 4.25], threshold=40.0, snr=False)
     assert np.array_equal(hits_abs, oracle.findprotohits(mats, 40.0))
+
+
+@pytest.mark.parametrize("Nf,Nt,r0,dr,Nr,blocks", [
+    (2 ** 16, 16, -8.0, 1 / 16, 256, [5, 0, 31, 3, 3]),
+    (2 ** 12, 7, -2.0, 0.25, 24, [2, 0]),
+    (2 ** 15, 32, -4.0, 1 / 16, 128, [15, 1, 8]),
+    (2 ** 20, 16, -8.0, 1 / 16, 256, [0, 17, 18, 31])])
+def test_rate_blocks_match_full_run(fdr, oracle, Nf, Nt, r0, dr, Nr, blocks):
+    """zdtfdr over a subset of 8-rate blocks in one pass equals the same columns of the
+    full run bit for bit, and its proto-hit scan equals findprotohits of its columns."""
+    spec = _spec(oracle, Nf, Nt, seed=Nf + 7 * Nt, ntones=5)
+    ws = fdr.ZDTWorkspace(spec, r0, dr, Nr)
+    assert ws.fused
+    full = fdr.zdtfdr(ws).cpu().numpy()
+    dest = fdr.fortran_empty(Nf, 8 * len(blocks))
+    fdr.zdtfdr_blocks_(dest, ws, spec, blocks)
+    cols = [8 * b + u for b in blocks for u in range(8)]
+    got = dest.cpu().numpy()
+    assert np.array_equal(got, full[:, cols])
+    hits, thr = fdr.zdtfdr_blocks_protohits_(dest, ws, spec, blocks, threshold=8.0, snr=True,
+                                             return_threshold=True)
+    m, s = oracle.fdrstats(got)
+    thr_ref = 8.0 * float(np.float32(s)) + float(np.float32(m))
+    assert abs(thr - thr_ref) <= 1e-6 * thr_ref
+    assert np.array_equal(hits, oracle.findprotohits(got, thr))
+
+
+def test_rate_blocks_argument_errors(fdr, oracle):
+    spec = _spec(oracle, 4096, 16, seed=1)
+    ws = fdr.ZDTWorkspace(spec, -2.0, 0.25, 16)
+    with pytest.raises(fdr.FDRError):
+        fdr.zdtfdr_blocks_(fdr.fortran_empty(4096, 8), ws, spec, [2])  # rates 16..23 > Nr
+    with pytest.raises(fdr.FDRError):
+        fdr.zdtfdr_blocks_(fdr.fortran_empty(4096, 24), ws, spec, [0, 1, 0])  # > Nr/8 blocks
+    st = fdr.ZDTWorkspace(spec, -2.0, 0.25, 16, staged_only=True)
+    with pytest.raises(fdr.FDRError):
+        fdr.zdtfdr_blocks_(fdr.fortran_empty(4096, 8), st, spec, [0])

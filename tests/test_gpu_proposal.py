@@ -118,13 +118,13 @@ def test_window_search_all_windows_matches_full(fdr):
     Nf, Nt = 1 << 16, 16
     full = P.FullSearch(Nf, Nt)
     net = P.ProposalNet(nbins=Nf // 256, cin=P.input_channels(Nt, True), max_batch=2, lag=True)
-    srch = P.ProposalSearch(net, tau=0.0, Nf=Nf, Nt=Nt, full=full)
+    srch = P.ProposalSearch(net, tau=0.5, Nf=Nf, Nt=Nt, full=full)
     for seed in (101, 102, 103):
         spec, tones = P.synth_channel(seed, Nf, Nt, max_tones=3, snr=(10, 30))
         ref = full.hits(spec)
         h, nr, fb = srch.search(spec, np.ones(16))
         assert not fb and nr == 256
-        assert P.recall(h, ref) >= 0.999 and P.recall(ref, h) >= 0.999
+        assert np.array_equal(h, ref)  # same columns, same statistics
         # a subset of windows finds exactly the reference's hits inside them (up to the
         # threshold, which comes from the statistics of the windows that ran)
         w = np.unique(ref[:, 1] // 16) if len(ref) else np.array([], int)
