@@ -104,8 +104,9 @@ SIGNATURES = {
     "fdr_propose_create": (INT, [C.POINTER(P), INT, INT, INT, INT, INT, INT, C.c_uint64]),
     "fdr_propose_destroy": (INT, [P]),
     "fdr_propose_num_params": (INT, [P, C.POINTER(I64)]),
-    "fdr_propose_features": (INT, [P, I64, I64, INT, P, P]),
-    "fdr_propose_lag_features": (INT, [P, I64, I64, INT, INT, P, P]),
+    "fdr_propose_features": (INT, [P, I64, I64, INT, INT, P, P]),
+    "fdr_propose_lag_features": (INT, [P, I64, I64, INT, INT, INT, P, P]),
+    "fdr_propose_input": (INT, [P, I64, I64, INT, INT, INT, P, P]),
     "fdr_propose_forward": (INT, [P, P, INT, P, P]),
     "fdr_propose_gradients": (INT, [P, P, P, INT, P, P, P, P]),
     "fdr_propose_train_step": (INT, [P, P, P, INT, F32, P, P, P]),

@@ -63,10 +63,41 @@ int64_t nextprod(const int64_t* factors, int nfactors, int64_t n) {
   return best == INT64_MAX ? -1 : best;
 }
 
+// Stream-ordered scratch comes from a memory pool owned by the library, one per device, that
+// keeps up to kScratchKeep bytes reserved across synchronisations.  (The device's default pool
+// releases everything at each synchronisation, so every allocation after one maps fresh
+// memory, which costs tens of microseconds per call.)
+static constexpr uint64_t kScratchKeep = 256ull << 20;
+
+static int scratch_pool(cudaMemPool_t* out) {
+  static std::mutex mu;
+  static cudaMemPool_t pools[64] = {};
+  int dev = 0;
+  FDR_CUDA(cudaGetDevice(&dev));
+  FDR_CHECK_ARG(dev >= 0 && dev < 64, "device ordinal %d out of range", dev);
+  std::lock_guard<std::mutex> lock(mu);
+  if (!pools[dev]) {
+    cudaMemPoolProps props;
+    memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    FDR_CUDA(cudaMemPoolCreate(&pool, &props));
+    uint64_t keep = kScratchKeep;
+    FDR_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    pools[dev] = pool;
+  }
+  *out = pools[dev];
+  return FDR_OK;
+}
+
 int scratch_alloc(void** p, size_t bytes, cudaStream_t s) {
   *p = nullptr;
   if (bytes == 0) return FDR_OK;
-  FDR_CUDA(cudaMallocAsync(p, bytes, s));
+  cudaMemPool_t pool = nullptr;
+  FDR_TRY(scratch_pool(&pool));
+  FDR_CUDA(cudaMallocFromPoolAsync(p, bytes, pool, s));
   return FDR_OK;
 }
 

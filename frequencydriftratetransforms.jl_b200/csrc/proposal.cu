@@ -53,74 +53,116 @@ struct fdr_propose_net {
 namespace fdr {
 
 // --------------------------------------------------------------------------------------
-// Features: out[t][bin] = (sum_{i < factor} spec[bin*factor + i, t] - factor) / sqrt(factor)
-// (exponential(1) background -> zero mean, unit variance).  One CTA of 256 threads per (bin, t).
+// Network input, one pass over the spectrogram.  For bin b (channels n = b*factor + i,
+// i < factor) and x = s - 1 (zero mean for an exponential(1) background):
+//   power[t][b] = sum_i x[n, t] / sqrt(factor)
+//   lag[l + ML][b] = sum_i sum_{t < Nt-1} x[n, t] * x[(n + l) mod Nf, t+1] / sqrt(factor*(Nt-1))
+// each optionally compressed to sign(v)*log1p(|v|).  One CTA of 256 threads per bin; the
+// bin's channels plus a halo of ML either side are staged in shared memory for `chunk`+1
+// steps at a time (all loads of a chunk in flight together); every block reduction runs in
+// a fixed order.
 // --------------------------------------------------------------------------------------
-__global__ void downsample_kernel(const float* __restrict__ spec, long long Nf, int Nt, int factor,
-                                  int nbins, float* __restrict__ out) {
-  const int bin = blockIdx.x, t = blockIdx.y;
-  const float* col = spec + (long long)t * Nf + (long long)bin * factor;
-  float s = 0.f;
-  for (int i = threadIdx.x; i < factor; i += blockDim.x) s += col[i];
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-  __shared__ float ws[32];
-  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+constexpr int kFeatThreads = 256;
+constexpr int kFeatMaxNt = 64;
+
+__device__ __forceinline__ float compress_value(float v, int compress) {
+  return compress ? copysignf(log1pf(fabsf(v)), v) : v;
+}
+
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <int ML>
+__global__ void __launch_bounds__(kFeatThreads)
+proposal_input_kernel(const float* __restrict__ spec, long long Nf, int Nt, int factor, int nbins,
+                      int chunk, float pscale, float lscale, int compress,
+                      float* __restrict__ pow_out, float* __restrict__ lag_out) {
+  constexpr int NL = 2 * ML + 1;
+  constexpr int NW = kFeatThreads / 32;
+  extern __shared__ float tile[];  // (chunk + 1) rows of W floats
+  __shared__ float red_p[kFeatMaxNt][NW];
+  __shared__ float red_l[NL][NW];
+  const int W = factor + 2 * ML;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int bin = blockIdx.x;
+  const long long n0 = (long long)bin * factor;
+  float lacc[NL];
+#pragma unroll
+  for (int l = 0; l < NL; ++l) lacc[l] = 0.f;
+  for (int t0 = 0; t0 < Nt; t0 += chunk) {
+    const int tc = min(chunk, Nt - t0);       // steps summed in this chunk
+    const int rows = min(tc + 1, Nt - t0);    // plus the next step for the lag products
+    __syncthreads();                          // the tile is free
+    for (int r = 0; r < rows; ++r) {
+      const float* col = spec + (long long)(t0 + r) * Nf;
+      for (int i = tid; i < W; i += kFeatThreads) {
+        long long n = n0 - ML + i;
+        n = n < 0 ? n + Nf : (n >= Nf ? n - Nf : n);
+        tile[r * W + i] = __ldg(col + n) - 1.f;
+      }
+    }
+    __syncthreads();
+    for (int r = 0; r < tc; ++r) {
+      const float* xr = tile + r * W + ML;
+      if (pow_out) {
+        float ps = 0.f;
+        for (int i = tid; i < factor; i += kFeatThreads) ps += xr[i];
+        ps = warp_sum(ps);
+        if (lane == 0) red_p[t0 + r][warp] = ps;
+      }
+      if (lag_out && r + 1 < rows) {
+        const float* xn = tile + (r + 1) * W;  // channel n0 - ML + i of step t+1
+        for (int i = tid; i < factor; i += kFeatThreads) {
+          const float a = xr[i];
+#pragma unroll
+          for (int l = 0; l < NL; ++l) lacc[l] = fmaf(a, xn[i + l], lacc[l]);
+        }
+      }
+    }
+  }
+  if (lag_out) {
+#pragma unroll
+    for (int l = 0; l < NL; ++l) {
+      const float v = warp_sum(lacc[l]);
+      if (lane == 0) red_l[l][warp] = v;
+    }
+  }
   __syncthreads();
-  if (threadIdx.x == 0) {
-    float tot = 0.f;
-    for (int i = 0; i < (int)(blockDim.x + 31) / 32; ++i) tot += ws[i];
-    out[(long long)t * nbins + bin] = (tot - (float)factor) * rsqrtf((float)factor);
+  if (pow_out && tid < Nt) {
+    float v = 0.f;
+    for (int w = 0; w < NW; ++w) v += red_p[tid][w];
+    pow_out[(long long)tid * nbins + bin] = compress_value(v * pscale, compress);
+  }
+  if (lag_out && tid < NL) {
+    float v = 0.f;
+    for (int w = 0; w < NW; ++w) v += red_l[tid][w];
+    lag_out[(long long)tid * nbins + bin] = compress_value(v * lscale, compress);
   }
 }
 
-// Lag products of adjacent steps, summed per bin (fdr_propose_lag_features).  One CTA per
-// bin; the bin's channels of step t and a halo of ML channels either side of step t+1 are
-// staged in shared memory; each thread owns channels i, i + blockDim, ... and keeps 2*ML+1
-// running sums; the per-lag block sums are reduced in a fixed order.
-template <int ML>
-__global__ void __launch_bounds__(256)
-lag_features_kernel(const float* __restrict__ spec, long long Nf, int Nt, int factor, int nbins,
-                    float scale, float* __restrict__ out) {
-  constexpr int NL = 2 * ML + 1;
-  extern __shared__ float sm[];
-  float* a = sm;                 // factor
-  float* b = sm + factor;        // factor + 2*ML
-  const int bin = blockIdx.x;
-  const long long n0 = (long long)bin * factor;
-  float acc[NL];
-#pragma unroll
-  for (int l = 0; l < NL; ++l) acc[l] = 0.f;
-  for (int t = 0; t + 1 < Nt; ++t) {
-    const float* c0 = spec + (long long)t * Nf;
-    const float* c1 = c0 + Nf;
-    __syncthreads();
-    for (int i = threadIdx.x; i < factor; i += blockDim.x) a[i] = c0[n0 + i] - 1.f;
-    for (int i = threadIdx.x; i < factor + 2 * ML; i += blockDim.x) {
-      long long n = n0 - ML + i;
-      n = n < 0 ? n + Nf : (n >= Nf ? n - Nf : n);
-      b[i] = c1[n] - 1.f;
-    }
-    __syncthreads();
-    for (int i = threadIdx.x; i < factor; i += blockDim.x) {
-      const float ai = a[i];
-#pragma unroll
-      for (int l = 0; l < NL; ++l) acc[l] = fmaf(ai, b[i + l], acc[l]);
-    }
-  }
-  __shared__ float red[NL][8];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-#pragma unroll
-  for (int l = 0; l < NL; ++l) {
-    float v = acc[l];
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if (lane == 0) red[l][warp] = v;
-  }
-  __syncthreads();
-  if (threadIdx.x < NL) {
-    float v = 0.f;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[threadIdx.x][w];
-    out[(long long)threadIdx.x * nbins + bin] = v * scale;
-  }
+static int launch_input(const float* spec, int64_t Nf, int64_t Nt, int factor, int maxlag,
+                        int compress, float* pow_out, float* lag_out, cudaStream_t s,
+                        const char* who) {
+  FDR_CHECK_ARG(spec != nullptr && (pow_out || lag_out), "%s: NULL argument", who);
+  FDR_CHECK_ARG(maxlag == 8, "%s: this build supports maxlag 8", who);
+  FDR_CHECK_ARG(factor >= 1 && factor <= 4096 && Nf % factor == 0 && Nf >= 2 * maxlag + 1 &&
+                Nf / factor <= 0x7fffffff,
+                "%s: Nf must be a multiple of factor (<= 4096) and >= %d", who, 2 * maxlag + 1);
+  FDR_CHECK_ARG(Nt >= 1 && Nt <= kFeatMaxNt && (lag_out == nullptr || Nt >= 2),
+                "%s: Nt must be in [1, %d] (>= 2 for lag products)", who, kFeatMaxNt);
+  const int nbins = (int)(Nf / factor);
+  const int W = factor + 2 * maxlag;
+  const int chunk = std::max(1, std::min(16, (int)((48 * 1024 / sizeof(float)) / W) - 1));
+  const size_t sm = sizeof(float) * (size_t)(chunk + 1) * W;
+  const float pscale = 1.f / sqrtf((float)factor);
+  const float lscale = Nt >= 2 ? 1.f / sqrtf((float)factor * (float)(Nt - 1)) : 0.f;
+  proposal_input_kernel<8><<<nbins, kFeatThreads, sm, s>>>(spec, Nf, (int)Nt, factor, nbins, chunk,
+                                                           pscale, lscale, compress, pow_out, lag_out);
+  FDR_LAUNCH_CHECK("proposal_input_kernel");
+  return FDR_OK;
 }
 
 // --------------------------------------------------------------------------------------
@@ -510,32 +552,23 @@ int fdr_propose_num_params(const fdr_propose_net* n, int64_t* count) {
   return FDR_OK;
 }
 
-int fdr_propose_features(const float* spec, int64_t Nf, int64_t Nt, int factor, float* out,
-                         fdr_stream_t stream) {
-  FDR_CHECK_ARG(spec && out, "fdr_propose_features: NULL argument");
-  FDR_CHECK_ARG(factor >= 1 && Nf % factor == 0 && Nt >= 1 && Nt <= 65535,
-                "fdr_propose_features: Nf must be a multiple of factor");
-  const int nbins = (int)(Nf / factor);
-  downsample_kernel<<<dim3(nbins, (unsigned)Nt), 256, 0, (cudaStream_t)stream>>>(spec, Nf, (int)Nt,
-                                                                                factor, nbins, out);
-  FDR_LAUNCH_CHECK("downsample_kernel");
-  return FDR_OK;
+int fdr_propose_features(const float* spec, int64_t Nf, int64_t Nt, int factor, int compress,
+                         float* out, fdr_stream_t stream) {
+  return launch_input(spec, Nf, Nt, factor, 8, compress, out, nullptr, (cudaStream_t)stream,
+                      "fdr_propose_features");
 }
 
 int fdr_propose_lag_features(const float* spec, int64_t Nf, int64_t Nt, int factor, int maxlag,
-                             float* out, fdr_stream_t stream) {
-  FDR_CHECK_ARG(spec && out, "fdr_propose_lag_features: NULL argument");
-  FDR_CHECK_ARG(maxlag == 8, "fdr_propose_lag_features: this build supports maxlag 8");
-  FDR_CHECK_ARG(factor >= 1 && factor <= 4096 && Nf % factor == 0 && Nf >= 2 * maxlag + 1 &&
-                Nt >= 2 && Nf / factor <= 0x7fffffff,
-                "fdr_propose_lag_features: Nf must be a multiple of factor (<= 4096), Nt >= 2");
-  const int nbins = (int)(Nf / factor);
-  const size_t sm = sizeof(float) * (2 * (size_t)factor + 2 * maxlag);
-  const float scale = 1.f / sqrtf((float)factor * (float)(Nt - 1));
-  lag_features_kernel<8><<<nbins, 256, sm, (cudaStream_t)stream>>>(spec, Nf, (int)Nt, factor, nbins,
-                                                                   scale, out);
-  FDR_LAUNCH_CHECK("lag_features_kernel");
-  return FDR_OK;
+                             int compress, float* out, fdr_stream_t stream) {
+  return launch_input(spec, Nf, Nt, factor, maxlag, compress, nullptr, out, (cudaStream_t)stream,
+                      "fdr_propose_lag_features");
+}
+
+int fdr_propose_input(const float* spec, int64_t Nf, int64_t Nt, int factor, int maxlag,
+                      int compress, float* out, fdr_stream_t stream) {
+  FDR_CHECK_ARG(out != nullptr, "fdr_propose_input: NULL argument");
+  return launch_input(spec, Nf, Nt, factor, maxlag, compress, out,
+                      out + Nt * (Nf / std::max(factor, 1)), (cudaStream_t)stream, "fdr_propose_input");
 }
 
 int fdr_propose_forward(fdr_propose_net* n, const float* x, int batch, float* logits,

@@ -450,10 +450,13 @@ static int zdt_execute_blocks(fdr_zdt* ws, const float* spectrogram, const int32
                   "zdtfdr blocks: block %lld = %d outside the workspace's %lld rates", (long long)i,
                   (int)blocks[i], (long long)ws->Nr);
   FDR_CHECK_ARG(4 * nblocks <= ws->W_pairs, "zdtfdr blocks: more than Nr/8 blocks");
+  // the kernels take the rate index of each block's first rate
+  std::vector<int> base((size_t)nblocks);
+  for (int64_t i = 0; i < nblocks; ++i) base[(size_t)i] = 8 * (int)blocks[i];
   int* d_blk = nullptr;
   FDR_TRY(scratch_alloc((void**)&d_blk, sizeof(int) * nblocks, s));
-  int st = cuda_status(cudaMemcpyAsync(d_blk, blocks, sizeof(int) * nblocks, cudaMemcpyHostToDevice, s),
-                       "upload rate blocks");
+  const cudaError_t ce = cudaMemcpyAsync(d_blk, base.data(), sizeof(int) * nblocks, cudaMemcpyHostToDevice, s);
+  int st = ce == cudaSuccess ? FDR_OK : cuda_status(ce, "upload rate blocks");
   zdt_mark(ws, "start", s);
   if (st == FDR_OK && spectrogram) {
     st = fdr_zdt_input(ws, spectrogram, s);

@@ -50,12 +50,13 @@ def input_channels(Nt, lag):
 class ProposalNet:
     """Handle on a device-resident network (fdr_propose_create)."""
 
-    def __init__(self, nbins=4096, cin=16, max_batch=64, seed=1, lag=False):
+    def __init__(self, nbins=4096, cin=16, max_batch=64, seed=1, lag=False, compress=True):
         h = C.c_void_p()
         _lib.check(_lib.lib().fdr_propose_create(C.byref(h), nbins, cin, 32, 5, NWIN, max_batch,
                                                  C.c_uint64(seed)))
         self._h = h
-        self.nbins, self.cin, self.max_batch, self.seed, self.lag = nbins, cin, max_batch, seed, lag
+        self.nbins, self.cin, self.max_batch, self.seed = nbins, cin, max_batch, seed
+        self.lag, self.compress = lag, compress
         self.meta = {}
         n = C.c_int64()
         _lib.check(_lib.lib().fdr_propose_num_params(self._h, C.byref(n)))
@@ -130,7 +131,8 @@ class ProposalNet:
         st = self.get_state()
         hdr = {"format": "fdr_propose_net/1", "nbins": self.nbins, "cin": self.cin, "width": 32,
                "ksize": 5, "nwin": NWIN, "nparams": self.nparams, "step": st["step"],
-               "seed": self.seed, "lag": self.lag, "extra": dict(self.meta, **(extra or {}))}
+               "seed": self.seed, "lag": self.lag, "compress": self.compress,
+               "extra": dict(self.meta, **(extra or {}))}
         hb = json.dumps(hdr, sort_keys=True).encode()
         with open(path, "wb") as fh:
             fh.write(struct.pack("<Q", len(hb)))
@@ -153,14 +155,16 @@ class ProposalNet:
     def load(cls, path, max_batch=64):
         hdr, st = cls.read_checkpoint(path)
         net = cls(hdr["nbins"], hdr["cin"], max_batch=max_batch, seed=hdr["seed"],
-                  lag=hdr.get("lag", False))
+                  lag=hdr.get("lag", False), compress=hdr.get("compress", False))
         net.set_state(st)
         net.meta = hdr.get("extra", {})
         return net
 
 
-def features(spec, lag=False, factor=FACTOR, out=None, stream=None):
-    """Network input (cin, Nf/factor) of a column-major (Nf, Nt) CUDA spectrogram."""
+def features(spec, lag=False, compress=True, factor=FACTOR, out=None, stream=None):
+    """Network input (cin, Nf/factor) of a column-major (Nf, Nt) CUDA spectrogram: the
+    power rows, then (lag) the 17 lag-product rows, each value v compressed to
+    sign(v)*log1p(|v|) when ``compress``."""
     Nf, Nt = spec.shape
     nb = Nf // factor
     cin = input_channels(Nt, lag)
@@ -169,10 +173,12 @@ def features(spec, lag=False, factor=FACTOR, out=None, stream=None):
     if tuple(out.shape) != (cin, nb) or not out.is_contiguous():
         raise ValueError(f"features: out must be a contiguous ({cin}, {nb}) tensor")
     sh = stream_handle(stream)
-    _lib.check(_lib.lib().fdr_propose_features(ptr(spec), Nf, Nt, factor, ptr(out), sh))
+    cflag = 1 if compress else 0
     if lag:
-        _lib.check(_lib.lib().fdr_propose_lag_features(ptr(spec), Nf, Nt, factor, MAXLAG,
-                                                       ptr(out[Nt:]), sh))
+        _lib.check(_lib.lib().fdr_propose_input(ptr(spec), Nf, Nt, factor, MAXLAG, cflag,
+                                                ptr(out), sh))
+    else:
+        _lib.check(_lib.lib().fdr_propose_features(ptr(spec), Nf, Nt, factor, cflag, ptr(out), sh))
     return out
 
 
@@ -225,7 +231,7 @@ def window_hit_counts(hits):
     return np.bincount(np.asarray(hits)[:, 1] // RATES_PER_WIN, minlength=NWIN)[:NWIN]
 
 
-def make_batch(seeds, full, lag, Nf=1 << 20, Nt=16, out=None, keep_hits=False):
+def make_batch(seeds, full, lag, Nf=1 << 20, Nt=16, out=None, keep_hits=False, compress=True):
     """Features (B, cin, Nf/256), labels (B, 16) and per-window hit counts (B, 16) for the
     seeded channels ``seeds`` (labels: 1 where the full search finds a proto-hit)."""
     B = len(seeds)
@@ -236,7 +242,7 @@ def make_batch(seeds, full, lag, Nf=1 << 20, Nt=16, out=None, keep_hits=False):
     all_hits = []
     for i, sd in enumerate(seeds):
         spec, _ = synth_channel(int(sd), Nf, Nt)
-        features(spec, lag, out=X[i])
+        features(spec, lag, compress, out=X[i])
         h = full.hits(spec)
         counts[i] = window_hit_counts(h)
         if keep_hits:
@@ -250,24 +256,38 @@ def lr_at(step, total, lr):
     return lr * (0.05 + 0.95 * 0.5 * (1.0 + math.cos(math.pi * min(step, total) / max(1, total))))
 
 
-def train_online(net, nchannels, seed0, batch=64, lr=2e-3, full=None, Nf=1 << 20, Nt=16,
+def train_online(nets, nchannels, seed0, batch=64, lr=2e-3, full=None, Nf=1 << 20, Nt=16,
                  log=None, log_every=50, start_step=0):
-    """Train on ``nchannels`` fresh seeded channels (seed0, seed0+1, ...), one pass, a batch
-    of ``batch`` per Adam step.  Resumable: ``start_step`` skips the batches already seen."""
+    """Train one or more networks on ``nchannels`` fresh seeded channels (seed0, seed0+1, ...),
+    one pass, ``batch`` channels per Adam step; the labels (one full search per channel) are
+    shared, a network without ``lag`` reads the power rows only.  Resumable: ``start_step``
+    skips the batches already seen.  Returns the loss history [(step, loss per network)]."""
+    nets = list(nets) if isinstance(nets, (list, tuple)) else [nets]
     full = full or FullSearch(Nf, Nt)
     total = nchannels // batch
-    X = torch.empty((batch, net.cin, Nf // FACTOR), dtype=torch.float32, device="cuda")
+    compress = nets[0].compress
+    if any(n.compress != compress for n in nets):
+        raise ValueError("networks trained together share the feature compression")
+    X = torch.empty((batch, input_channels(Nt, True), Nf // FACTOR), dtype=torch.float32,
+                    device="cuda")
+    Xp = torch.empty((batch, Nt, Nf // FACTOR), dtype=torch.float32, device="cuda")
     hist = []
     t0 = time.time()
     for step in range(start_step, total):
         seeds = range(seed0 + step * batch, seed0 + (step + 1) * batch)
-        _, Y, _ = make_batch(seeds, full, net.lag, Nf, Nt, out=X)
-        loss = net.train_step(X, Y, lr_at(step, total, lr))
+        _, Y, _ = make_batch(seeds, full, True, Nf, Nt, out=X, compress=compress)
+        losses = []
+        for n in nets:
+            if n.lag:
+                losses.append(n.train_step(X, Y, lr_at(step, total, lr)))
+            else:
+                Xp.copy_(X[:, :Nt])
+                losses.append(n.train_step(Xp, Y, lr_at(step, total, lr)))
         if log_every and (step % log_every == 0 or step == total - 1):
-            lv = float(loss.item())
+            lv = [round(float(l.item()), 5) for l in losses]
             hist.append((step, lv))
             if log:
-                log(f"step {step}/{total} loss {lv:.4f} ({time.time() - t0:.0f} s)")
+                log(f"step {step}/{total} loss {lv} ({time.time() - t0:.0f} s)")
     torch.cuda.synchronize()
     return hist
 
@@ -306,7 +326,7 @@ class ProposalSearch:
         X = torch.empty((len(specs), self.net.cin, self.Nf // FACTOR), dtype=torch.float32,
                         device="cuda")
         for i, s in enumerate(specs):
-            features(s, self.net.lag, out=X[i])
+            features(s, self.net.lag, self.net.compress, out=X[i])
         return self.net.probabilities(X).cpu().numpy()
 
     def search(self, spec, p, snr=10.0):
@@ -335,30 +355,89 @@ def recall(hits, ref):
     return len(a & b) / len(b)
 
 
-def calibrate(probs, counts, target=0.997, win_cost=1.0, full_cost=None, max_windows=NWIN):
+def calibrate(probs, counts, target=0.997, fixed_cost=0.0, win_cost=1.0, full_cost=None,
+              max_windows=NWIN):
     """Pick (tau, tau_hi) on a validation set so that the proto-hits inside the windows that
     run (or in channels that fall back) are >= ``target`` of all proto-hits, at the least
-    cost (win_cost per window run, full_cost per fallback; defaults to 16 windows)."""
+    modelled cost: fixed_cost + win_cost per window for a channel whose windows run (nothing
+    when no window is proposed), full_cost for a fallback (default 16 windows)."""
     probs, counts = np.asarray(probs), np.asarray(counts)
-    full_cost = NWIN * win_cost if full_cost is None else full_cost
+    full_cost = fixed_cost + NWIN * win_cost if full_cost is None else full_cost
     total = counts.sum()
-    grid = np.unique(np.concatenate([[0.0], np.quantile(probs, np.linspace(0, 1, 201))]))
+    grid = np.unique(np.concatenate([[0.0, 1.0], np.quantile(probs, np.linspace(0, 1, 201))]))
     best = None
     for tau in grid:
         for tau_hi in grid[grid >= tau]:
             unc = np.any((probs >= tau) & (probs < tau_hi), axis=1)
             run = probs >= tau_hi
-            fb = unc | (run.sum(axis=1) > max_windows)
+            k = run.sum(axis=1)
+            fb = unc | (k > max_windows)
             found = np.where(fb, counts.sum(axis=1), (counts * run).sum(axis=1)).sum()
             rec = found / total if total else 1.0
             if rec < target:
                 continue
-            cost = np.where(fb, full_cost, run.sum(axis=1) * win_cost).sum()
+            cost = np.where(fb, full_cost, np.where(k > 0, fixed_cost + k * win_cost, 0.0)).sum()
             if best is None or cost < best[0]:
                 best = (float(cost), float(tau), float(tau_hi), float(rec), float(fb.mean()))
-            break  # larger tau_hi only adds fallbacks at this tau
-    if best is None:
-        return {"tau": 0.0, "tau_hi": 0.0, "cost": full_cost * len(probs), "window_recall": 1.0,
-                "fallback_rate": 0.0}
-    return {"cost": best[0], "tau": best[1], "tau_hi": best[2], "window_recall": best[3],
-            "fallback_rate": best[4]}
+            break  # a larger tau_hi only turns runs into fallbacks at this tau
+    return {"cost": best[0], "cost_frac": best[0] / (full_cost * len(probs)), "tau": best[1],
+            "tau_hi": best[2], "window_recall": best[3], "fallback_rate": best[4]}
+
+
+def measure_costs(full, spec, reps=10):
+    """Device-synchronised wall time (ms) of the full search and of window searches with 1
+    and 16 windows on one channel -> (fixed, per-window, full) of the calibration cost model."""
+    srch = ProposalSearch(None, tau=0.5, full=full)
+
+    def tm(f):
+        f()
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        for _ in range(reps):
+            f()
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t) / reps * 1e3
+
+    t_full = tm(lambda: full.hits(spec))
+    p1, p16 = np.zeros(NWIN), np.ones(NWIN)
+    p1[0] = 1.0
+    t1 = tm(lambda: srch.search(spec, p1))
+    t16 = tm(lambda: srch.search(spec, p16))
+    per = (t16 - t1) / (NWIN - 1)
+    return {"fixed_ms": t1 - per, "per_window_ms": per, "full_ms": t_full}
+
+
+def evaluate(net, specs, full, tau, tau_hi, snr=10.0, ref_hits=None):
+    """Proposal search over ``specs`` (resident CUDA spectrograms) against the full search:
+    proto-hit recall (pooled over channels), rates computed, fallbacks and the device-
+    synchronised wall time of both paths (the proposal path includes its features and
+    network inference; net=None proposes every window)."""
+    srch = ProposalSearch(net, tau=tau, tau_hi=tau_hi, full=full)
+    if ref_hits is None:
+        ref_hits = [full.hits(s, snr) for s in specs]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for s in specs:
+        full.hits(s, snr)
+    torch.cuda.synchronize()
+    t_full = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    if net is not None:
+        probs = srch.probabilities(specs)
+    else:
+        probs = np.ones((len(specs), NWIN))
+    out = [srch.search(s, p, snr) for s, p in zip(specs, probs)]
+    torch.cuda.synchronize()
+    t_prop = time.perf_counter() - t0
+    found = total = rates = fb = 0
+    for (h, nr, f), ref in zip(out, ref_hits):
+        total += len(ref)
+        if len(ref):
+            found += int(round(recall(h, ref) * len(ref)))
+        rates += nr
+        fb += int(f)
+    n = len(specs)
+    return {"channels": n, "recall": found / total if total else 1.0, "hits": total,
+            "rates_frac": rates / (n * NRATES), "fallback_frac": fb / n,
+            "full_ms_per_channel": t_full / n * 1e3, "proposal_ms_per_channel": t_prop / n * 1e3,
+            "speedup": t_full / t_prop}

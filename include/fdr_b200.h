@@ -215,16 +215,22 @@ int fdr_propose_create(fdr_propose_net** net, int nbins, int nt, int width, int 
 int fdr_propose_destroy(fdr_propose_net* net);
 int fdr_propose_num_params(const fdr_propose_net* net, int64_t* count);
 /* Network input of one spectrogram (Nf x Nt): out[t][bin] = (sum of `factor` consecutive
-   channels - factor) / sqrt(factor), bin < Nf/factor (device, Nt x Nf/factor row-major). */
+   channels - factor) / sqrt(factor), bin < Nf/factor (device, Nt x Nf/factor row-major);
+   with compress != 0 each value v is replaced by sign(v) * log1p(|v|).  Nt <= 64. */
 int fdr_propose_features(const float* spectrogram, int64_t Nf, int64_t Nt, int factor,
-                         float* out, fdr_stream_t stream);
+                         int compress, float* out, fdr_stream_t stream);
 /* Drift evidence of one spectrogram: out[l + maxlag][bin] = sum over the `factor` channels n
    of the bin and over t < Nt-1 of (s[n,t] - 1) * (s[(n + l) mod Nf, t+1] - 1), divided by
    sqrt(factor * (Nt - 1)), for lags l in [-maxlag, maxlag] (maxlag 8, factor <= 4096; device,
    (2*maxlag+1) x Nf/factor row-major).  Zero mean, unit variance for an exponential(1)
-   background; a tone drifting r channels per step shows up at lags floor(r) and ceil(r). */
+   background; a tone drifting r channels per step shows up at lags floor(r) and ceil(r).
+   compress as for fdr_propose_features. */
 int fdr_propose_lag_features(const float* spectrogram, int64_t Nf, int64_t Nt, int factor,
-                             int maxlag, float* out, fdr_stream_t stream);
+                             int maxlag, int compress, float* out, fdr_stream_t stream);
+/* Both in one pass: out rows 0..Nt-1 as fdr_propose_features, rows Nt..Nt+2*maxlag as
+   fdr_propose_lag_features (the input of a network with nt = Nt + 2*maxlag + 1). */
+int fdr_propose_input(const float* spectrogram, int64_t Nf, int64_t Nt, int factor, int maxlag,
+                      int compress, float* out, fdr_stream_t stream);
 /* logits[b][w] (device) for x[b][t][bin] (device), b < batch. */
 int fdr_propose_forward(fdr_propose_net* net, const float* x, int batch, float* logits,
                         fdr_stream_t stream);

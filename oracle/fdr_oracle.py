@@ -629,15 +629,20 @@ def propose_loss_and_grad(params, x, labels, nt, half_weights=True):
     return loss, np.concatenate(flat)
 
 
-def propose_features(spec, factor=256):
-    """Power input of the proposal net: (Nt, Nf/factor), (group sum - factor)/sqrt(factor)."""
+def _compress(v, compress):
+    return np.sign(v) * np.log1p(np.abs(v)) if compress else v
+
+
+def propose_features(spec, factor=256, compress=False):
+    """Power input of the proposal net: (Nt, Nf/factor), (group sum - factor)/sqrt(factor),
+    optionally compressed to sign(v)*log1p(|v|)."""
     s = np.asarray(spec, np.float64)
     Nf, Nt = s.shape
     g = s.reshape(Nf // factor, factor, Nt).sum(axis=1)
-    return ((g - factor) / math.sqrt(factor)).T
+    return _compress(((g - factor) / math.sqrt(factor)).T, compress)
 
 
-def propose_lag_features(spec, factor=256, maxlag=8):
+def propose_lag_features(spec, factor=256, maxlag=8, compress=False):
     """Drift evidence input: (2*maxlag+1, Nf/factor); row l+maxlag = per-bin sums over
     t < Nt-1 of (s[n,t]-1)(s[(n+l) mod Nf,t+1]-1), divided by sqrt(factor*(Nt-1))."""
     s = np.asarray(spec, np.float64) - 1.0
@@ -646,4 +651,4 @@ def propose_lag_features(spec, factor=256, maxlag=8):
     for li, l in enumerate(range(-maxlag, maxlag + 1)):
         prod = (s[:, :-1] * np.roll(s[:, 1:], -l, axis=0)).sum(axis=1)
         out[li] = prod.reshape(Nf // factor, factor).sum(axis=1)
-    return out / math.sqrt(factor * (Nt - 1))
+    return _compress(out / math.sqrt(factor * (Nt - 1)), compress)

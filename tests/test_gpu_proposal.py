@@ -17,16 +17,26 @@ def _exp_spec(rng, Nf, Nt):
     return (-np.log(rng.random((Nf, Nt)))).astype(np.float32)
 
 
-def test_features_match_oracle(fdr, oracle):
+@pytest.mark.parametrize("compress", [False, True])
+def test_features_match_oracle(fdr, oracle, compress):
     rng = np.random.default_rng(11)
     Nf, Nt = 1 << 14, 16
     spec = _exp_spec(rng, Nf, Nt)
     spec[1000:1016, :] += 30.0  # structure in a few bins
     d = fdr.arrays.as_device_f32(spec)
-    x = fdr.proposal.features(d, lag=True).cpu().numpy()
-    ref_p = oracle.propose_features(spec)
-    ref_l = oracle.propose_lag_features(spec)
+    x = fdr.proposal.features(d, lag=True, compress=compress).cpu().numpy()
+    ref_p = oracle.propose_features(spec, compress=compress)
+    ref_l = oracle.propose_lag_features(spec, compress=compress)
     assert x.shape == (Nt + 17, Nf // 256)
+    # the power-only and lag-only entry points give the same rows
+    xp = fdr.proposal.features(d, lag=False, compress=compress).cpu().numpy()
+    assert np.array_equal(xp, x[:Nt])
+    import torch as _t
+    xl = _t.empty((17, Nf // 256), dtype=_t.float32, device="cuda")
+    fdr._lib.check(fdr._lib.lib().fdr_propose_lag_features(
+        fdr.arrays.ptr(d), Nf, Nt, 256, 8, int(compress), fdr.arrays.ptr(xl),
+        fdr.arrays.stream_handle()))
+    assert np.array_equal(xl.cpu().numpy(), x[Nt:])
     assert np.max(np.abs(x[:Nt] - ref_p)) < 2e-4 * max(1.0, np.max(np.abs(ref_p)))
     assert np.max(np.abs(x[Nt:] - ref_l)) < 2e-4 * max(1.0, np.max(np.abs(ref_l)))
 
