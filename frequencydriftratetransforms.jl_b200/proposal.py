@@ -355,33 +355,39 @@ def recall(hits, ref):
     return len(a & b) / len(b)
 
 
-def calibrate(probs, counts, target=0.997, fixed_cost=0.0, win_cost=1.0, full_cost=None,
-              max_windows=NWIN):
-    """Pick (tau, tau_hi) on a validation set so that the proto-hits inside the windows that
-    run (or in channels that fall back) are >= ``target`` of all proto-hits, at the least
-    modelled cost: fixed_cost + win_cost per window for a channel whose windows run (nothing
-    when no window is proposed), full_cost for a fallback (default 16 windows)."""
-    probs, counts = np.asarray(probs), np.asarray(counts)
+def calibrate(probs, counts, target=0.997, fixed_cost=0.0, win_cost=1.0, full_cost=None):
+    """Pick (tau, tau_hi, max_windows) on a validation set so that the proto-hits inside the
+    windows that run (or in channels that fall back) are >= ``target`` of all proto-hits, at
+    the least modelled cost: fixed_cost + win_cost per window for a channel whose windows
+    run (nothing when no window is proposed), full_cost for a fallback (default: 16 windows).
+    A channel falls back when a window is uncertain (tau <= p < tau_hi) or when more than
+    max_windows windows would run."""
+    probs, counts = np.asarray(probs, np.float64), np.asarray(counts)
     full_cost = fixed_cost + NWIN * win_cost if full_cost is None else full_cost
     total = counts.sum()
+    ch_hits = counts.sum(axis=1)
     grid = np.unique(np.concatenate([[0.0, 1.0], np.quantile(probs, np.linspace(0, 1, 201))]))
     best = None
     for tau in grid:
+        above = probs >= tau
         for tau_hi in grid[grid >= tau]:
-            unc = np.any((probs >= tau) & (probs < tau_hi), axis=1)
             run = probs >= tau_hi
+            unc = np.any(above & ~run, axis=1)
             k = run.sum(axis=1)
-            fb = unc | (k > max_windows)
-            found = np.where(fb, counts.sum(axis=1), (counts * run).sum(axis=1)).sum()
-            rec = found / total if total else 1.0
-            if rec < target:
-                continue
-            cost = np.where(fb, full_cost, np.where(k > 0, fixed_cost + k * win_cost, 0.0)).sum()
-            if best is None or cost < best[0]:
-                best = (float(cost), float(tau), float(tau_hi), float(rec), float(fb.mean()))
-            break  # a larger tau_hi only turns runs into fallbacks at this tau
+            in_run = (counts * run).sum(axis=1)
+            for kmax in range(NWIN + 1):
+                fb = unc | (k > kmax)
+                found = np.where(fb, ch_hits, in_run).sum()
+                rec = found / total if total else 1.0
+                if rec < target:
+                    continue
+                cost = np.where(fb, full_cost, np.where(k > 0, fixed_cost + k * win_cost, 0.0)).sum()
+                if best is None or cost < best[0]:
+                    best = (float(cost), float(tau), float(tau_hi), int(kmax), float(rec),
+                            float(fb.mean()))
     return {"cost": best[0], "cost_frac": best[0] / (full_cost * len(probs)), "tau": best[1],
-            "tau_hi": best[2], "window_recall": best[3], "fallback_rate": best[4]}
+            "tau_hi": best[2], "max_windows": best[3], "window_recall": best[4],
+            "fallback_rate": best[5]}
 
 
 def measure_costs(full, spec, reps=10):
@@ -407,12 +413,12 @@ def measure_costs(full, spec, reps=10):
     return {"fixed_ms": t1 - per, "per_window_ms": per, "full_ms": t_full}
 
 
-def evaluate(net, specs, full, tau, tau_hi, snr=10.0, ref_hits=None):
+def evaluate(net, specs, full, tau, tau_hi, snr=10.0, ref_hits=None, max_windows=NWIN):
     """Proposal search over ``specs`` (resident CUDA spectrograms) against the full search:
     proto-hit recall (pooled over channels), rates computed, fallbacks and the device-
     synchronised wall time of both paths (the proposal path includes its features and
     network inference; net=None proposes every window)."""
-    srch = ProposalSearch(net, tau=tau, tau_hi=tau_hi, full=full)
+    srch = ProposalSearch(net, tau=tau, tau_hi=tau_hi, max_windows=max_windows, full=full)
     if ref_hits is None:
         ref_hits = [full.hits(s, snr) for s in specs]
     torch.cuda.synchronize()

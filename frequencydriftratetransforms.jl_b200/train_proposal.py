@@ -39,6 +39,8 @@ def main(argv=None):
     ap.add_argument("--target", type=float, default=0.998, help="calibration recall target")
     ap.add_argument("--out-dir", default=os.path.join(HERE, "data"))
     ap.add_argument("--report", default=None)
+    ap.add_argument("--eval-only", default=None, metavar="DIR",
+                    help="skip training: load proposal_lag.bin / proposal_power.bin from DIR")
     a = ap.parse_args(argv)
     os.makedirs(a.out_dir, exist_ok=True)
     full = P.FullSearch()
@@ -47,8 +49,14 @@ def main(argv=None):
             "power": P.ProposalNet(4096, 16, max_batch=max(a.batch, 64), seed=a.seed, lag=False)}
     untrained = {"lag": P.ProposalNet(4096, cin_lag, max_batch=64, seed=a.seed, lag=True)}
     t0 = time.time()
-    hist = P.train_online([nets["lag"], nets["power"]], a.channels, 1_000_000, batch=a.batch,
-                          lr=a.lr, full=full, log=lambda m: print(m, flush=True), log_every=200)
+    if a.eval_only:
+        nets = {k: P.ProposalNet.load(os.path.join(a.eval_only, f"proposal_{k}.bin"), max_batch=64)
+                for k in ("lag", "power")}
+        hist = []
+        a.channels = nets["lag"].meta.get("train_channels", a.channels)
+    else:
+        hist = P.train_online([nets["lag"], nets["power"]], a.channels, 1_000_000, batch=a.batch,
+                              lr=a.lr, full=full, log=lambda m: print(m, flush=True), log_every=200)
     train_s = time.time() - t0
     # calibration set
     vseeds = range(2_000_000_000, 2_000_000_000 + a.val)
@@ -68,11 +76,13 @@ def main(argv=None):
         probs = net.probabilities(x).cpu().numpy()
         cal = P.calibrate(probs, cv, target=a.target, fixed_cost=costs["fixed_ms"],
                           win_cost=costs["per_window_ms"], full_cost=costs["full_ms"])
-        res = P.evaluate(net, specs, full, cal["tau"], cal["tau_hi"], ref_hits=ref)
+        res = P.evaluate(net, specs, full, cal["tau"], cal["tau_hi"], ref_hits=ref,
+                         max_windows=cal["max_windows"])
         report[name] = {"calibration": cal, "test": res}
         print(name, json.dumps(report[name]), flush=True)
         if name in nets:
-            net.meta = {"tau": cal["tau"], "tau_hi": cal["tau_hi"], "calibration": cal,
+            net.meta = {"tau": cal["tau"], "tau_hi": cal["tau_hi"],
+                        "max_windows": cal["max_windows"], "calibration": cal,
                         "test": res, "train_channels": a.channels, "costs": costs}
             net.save(os.path.join(a.out_dir, f"proposal_{name}.bin"))
     print(json.dumps(report), flush=True)
