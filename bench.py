@@ -59,6 +59,63 @@ def algorithmic_bytes():
     return 4 * NF * NT + 4 * NF * NR
 
 
+# DRAM bytes (read + write) of one fused zdtfdr! call at this workload, summed over its three
+# kernels from one ncu capture (profiles/zdt_kernels_traffic_Nf2e20_Nt16_Nr129.md).
+NCU_TRAFFIC_PER_CALL = None
+
+
+def nominal_flops():
+    """Nominal FLOP count of one ZDT call: 2.5*Nf*log2(Nf)*(Nt+Nr) for the real FFTs plus
+    K*(10*Nl*log2(Nl) + 6*(Nt+Nl+Nr)) for the chirp-z convolution (K = Nf/2+1)."""
+    Nl = 144
+    K = NF // 2 + 1
+    return 2.5 * NF * math.log2(NF) * (NT + NR) + K * (10 * Nl * math.log2(Nl) + 6 * (NT + Nl + NR))
+
+
+def fp32_peak_tflops(torch):
+    """FP32 FMA throughput measured by a cuBLAS SGEMM (TF32 off), TFLOP/s."""
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        n = 8192
+        a = torch.randn((n, n), device="cuda")
+        b = torch.randn((n, n), device="cuda")
+        for _ in range(2):
+            a @ b
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(5):
+            a @ b
+        e1.record()
+        e1.synchronize()
+        return 2.0 * n ** 3 * 5 / (e0.elapsed_time(e1) * 1e-3) / 1e12
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+
+
+def proposal_leg(fdr, torch, nchan=64):
+    """Learned rate-window proposal on held-out synthetic channels (Nf=2^20, Nt=16, 0-5 tones
+    of amplitude 8-40, rates in [-8, 8]): the trained network (power + lag input) at its
+    calibrated thresholds against the full 256-rate search, both with findprotohits at SNR 10."""
+    P = fdr.proposal
+    ckpt = os.path.join(ROOT, "frequencydriftratetransforms.jl_b200", "data", "proposal_lag.bin")
+    if not os.path.exists(ckpt):
+        return None
+    net = P.ProposalNet.load(ckpt, max_batch=64)
+    full = P.FullSearch()
+    specs = [P.synth_channel(3_000_000_000 + i)[0] for i in range(nchan)]
+    P.evaluate(net, specs[:4], full, net.meta["tau"], net.meta["tau_hi"],
+               max_windows=net.meta.get("max_windows", 16))  # warm-up
+    res = P.evaluate(net, specs, full, net.meta["tau"], net.meta["tau_hi"],
+                     max_windows=net.meta.get("max_windows", 16))
+    res["workload"] = ("held-out channels Nf=2^20 x Nt=16, 0-5 tones SNR 8-40, rates -8..8, "
+                       "16 windows of 16 rates; times include features and inference")
+    res["train_channels"] = net.meta.get("train_channels")
+    del specs
+    return res
+
+
 class ClockSampler:
     """nvidia-smi clocks/throttle sampling during the timed region."""
 
@@ -221,6 +278,10 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched multi-channel leg (64 uneven coarse channels)")
+    ap.add_argument("--no-proposal", action="store_true",
+                    help="skip the learned rate-window proposal leg")
+    ap.add_argument("--no-fp32-peak", action="store_true",
+                    help="skip the SGEMM measurement of the FP32 peak (compute.frac)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -350,6 +411,11 @@ def main():
     batched = None
     if not args.no_batched:
         batched = batched_leg(fdr, torch, max(3, min(args.steps, 10)))
+    proposal = None
+    if rank == 0 and not args.no_proposal:
+        proposal = proposal_leg(fdr, torch)
+    fp32_peak = fp32_peak_tflops(torch) if rank == 0 and not args.no_fp32_peak else None
+    flops = nominal_flops()
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -377,13 +443,18 @@ def main():
                             "zdtfdr! with fused findprotohits(snr=10) -> hits to host"},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak, "traffic": NCU_TRAFFIC_PER_CALL,
                          "kernel": "whole ZDT call (all launches of one zdtfdr!)",
                          "algorithmic_bytes": algorithmic_bytes(), "peak_source": peak_src},
+            "compute": {"flop_nominal": flops, "achieved_tflops": flops / (ms_step * 1e-3) / 1e12,
+                        "fp32_peak_tflops": fp32_peak,
+                        "frac": (flops / (ms_step * 1e-3) / 1e12) / fp32_peak if fp32_peak else None,
+                        "peak_source": "cuBLAS SGEMM 8192^3 (TF32 off) measured in this run"},
             "stages_ms": stages,
             "clocks": clk,
             "cpu_baseline": cpu,
             "batched": batched,
+            "proposal": proposal,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

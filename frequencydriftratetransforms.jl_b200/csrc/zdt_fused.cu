@@ -229,6 +229,29 @@ __device__ __forceinline__ float2 horner(const float2 (&G)[NTR], float2 w) {
   return s;
 }
 
+// Packed-FP32 helpers (sm_100 FFMA2 / FMUL2): lane 0 and lane 1 carry two independent
+// evaluations, each lane performing exactly the scalar operation sequence.
+__device__ __forceinline__ float2 pk_fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 pk_mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 pk_neg(float2 a) { return __fmul2_rn(a, make_float2(-1.f, -1.f)); }
+
+// horner() for the two bins of a thread at once: (Gx[t], Gy[t]) hold the real and imaginary
+// parts of F[k_b, t] for b = 0, 1 in the two lanes; (wx, wy) the two multipliers.
+template <int NTR>
+__device__ __forceinline__ void horner_pk(const float2 (&Gx)[NTR], const float2 (&Gy)[NTR], float2 wx,
+                                          float2 wy, float2& sx, float2& sy) {
+  const float2 nwy = pk_neg(wy);
+  sx = Gx[NTR - 1];
+  sy = Gy[NTR - 1];
+#pragma unroll
+  for (int t = NTR - 2; t >= 0; --t) {
+    const float2 tx = pk_fma(sx, wx, pk_fma(sy, nwy, Gx[t]));
+    const float2 ty = pk_fma(sx, wy, pk_fma(sy, wx, Gy[t]));
+    sx = tx;
+    sy = ty;
+  }
+}
+
 __device__ __forceinline__ float window_value(const CztArgs& a, long long k) {
   if (a.window == FDR_WINDOW_HAMMING) return (float)(0.53836 + 0.46164 * cospi(2.0 * (double)k / (double)a.N));
   if (a.window == FDR_WINDOW_CUSTOM) return (float)a.wk[k];
@@ -257,23 +280,35 @@ __global__ void __launch_bounds__(Q / 2, 1) zdtf_czt_kernel(CztArgs a) {
     const int side = i / Q, na = i - side * Q;
     twr[i] = cscale(cconj(tw_fwd(a.tab, (long long)k1s[side] * na)), invN);
   }
-  float2 G[2][NTR];
-  czt_forward<Q, NTR>(a, c, k1s, buf, twt, gnyq, G);
+  float2 Gx[NTR], Gy[NTR];  // lanes = the thread's two bins
+  {
+    float2 G[2][NTR];
+    czt_forward<Q, NTR>(a, c, k1s, buf, twt, gnyq, G);
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) {
+      Gx[t] = make_float2(G[0][t].x, G[1][t].x);
+      Gy[t] = make_float2(G[0][t].y, G[1][t].y);
+    }
+  }
 
   // Per-base phase state: w_{k,j} = exp(2 pi i (alpha + j*beta) / 2^bits); rates are taken
   // kHorner at a time, w = w(first rate of the group, exact) * pw[jr] (exact).
   const unsigned long long mask = a.ph.mask;
   unsigned long long alpha[2], beta[2];
-  float2 pw[2][kHorner + 1];  // exact w(k, i*dr) for i < kHorner, and for i = kHorner
-  float win[2];
+  float2 PWx[kHorner + 1], PWy[kHorner + 1];  // exact w(k_b, i*dr), lanes = b
+  float2 WIN;
 #pragma unroll
   for (int b = 0; b < 2; ++b) {
     const unsigned long long k = (unsigned long long)k1s[b] + (unsigned long long)P * tid;
     alpha[b] = (k * a.ph.R0) & mask;
     beta[b] = (k * a.ph.Rd) & mask;
 #pragma unroll
-    for (int i = 0; i <= kHorner; ++i) pw[b][i] = cis_phase(((unsigned long long)i * beta[b]) & mask, a.ph);
-    win[b] = window_value(a, (long long)k);
+    for (int i = 0; i <= kHorner; ++i) {
+      const float2 p = cis_phase(((unsigned long long)i * beta[b]) & mask, a.ph);
+      if (b == 0) { PWx[i].x = p.x; PWy[i].x = p.y; } else { PWx[i].y = p.x; PWy[i].y = p.y; }
+    }
+    const float wv = window_value(a, (long long)k);
+    if (b == 0) WIN.x = wv; else WIN.y = wv;
   }
   // Nyquist bin (CTA 0, thread 0)
   const unsigned long long kny = (unsigned long long)(a.N / 2);
@@ -291,23 +326,34 @@ __global__ void __launch_bounds__(Q / 2, 1) zdtf_czt_kernel(CztArgs a) {
     const long long jg = a.blk_base ? (long long)__ldg(a.blk_base + (q0 >> 2)) : (long long)j0;
     __syncthreads();  // buf is free
     // exact phase of the block's first rate; the second half starts at w0 * w(k, 4*dr)
-    float2 wb[2];
-#pragma unroll
-    for (int b = 0; b < 2; ++b) wb[b] = cis_phase((alpha[b] + (unsigned long long)jg * beta[b]) & mask, a.ph);
+    float2 Wbx, Wby;
+    {
+      const float2 w0 = cis_phase((alpha[0] + (unsigned long long)jg * beta[0]) & mask, a.ph);
+      const float2 w1 = cis_phase((alpha[1] + (unsigned long long)jg * beta[1]) & mask, a.ph);
+      Wbx = make_float2(w0.x, w1.x);
+      Wby = make_float2(w0.y, w1.y);
+    }
 #pragma unroll
     for (int h = 0; h < kRatesPerBlock / kHorner; ++h) {
       const int jh = j0 + h * kHorner;
       float2 S[2][kHorner];
+      float2 W0x = Wbx, W0y = Wby;
+      if (h > 0) {  // w(first rate of the half) = wb * w(k, kHorner*dr)
+        W0x = pk_fma(Wbx, PWx[kHorner], pk_mul(pk_neg(Wby), PWy[kHorner]));
+        W0y = pk_fma(Wbx, PWy[kHorner], pk_mul(Wby, PWx[kHorner]));
+      }
+      const float2 NW0y = pk_neg(W0y);
 #pragma unroll
-      for (int b = 0; b < 2; ++b) {
-        const float2 w0 = (h == 0) ? wb[b] : cmul(wb[b], pw[b][kHorner]);
-#pragma unroll
-        for (int jr = 0; jr < kHorner; ++jr) {
-          const float2 w = cmul(w0, pw[b][jr]);
-          float2 sv = horner<NTR>(G[b], w);
-          if (jh + jr >= a.Nr) sv = make_float2(0.f, 0.f);
-          S[b][jr] = cscale(sv, win[b]);
-        }
+      for (int jr = 0; jr < kHorner; ++jr) {
+        const float2 wx = pk_fma(W0x, PWx[jr], pk_mul(NW0y, PWy[jr]));
+        const float2 wy = pk_fma(W0x, PWy[jr], pk_mul(W0y, PWx[jr]));
+        float2 sx, sy;
+        horner_pk<NTR>(Gx, Gy, wx, wy, sx, sy);
+        sx = pk_mul(sx, WIN);
+        sy = pk_mul(sy, WIN);
+        const bool live = jh + jr < a.Nr;
+        S[0][jr] = live ? make_float2(sx.x, sy.x) : make_float2(0.f, 0.f);
+        S[1][jr] = live ? make_float2(sx.y, sy.y) : make_float2(0.f, 0.f);
       }
 #pragma unroll
       for (int b = 0; b < 2; ++b) {
@@ -473,18 +519,37 @@ __global__ void __launch_bounds__(CztSmemShape<Q>::T, 1) zdtf_czt_smem_kernel(Cz
     const int j0 = 2 * q0 + g * RPT;  // this thread's first rate of the block
     const long long jb = a.blk_base ? (long long)__ldg(a.blk_base + (q0 >> 2)) : (long long)(2 * q0);
     const float2 w0 = cis_phase((alpha + (unsigned long long)(jb + g * RPT) * beta) & mask, a.ph);
-    float2 w[RPT], S[RPT];
+    // Horner's rule for the RPT rates, two rates per packed-FP32 lane pair
+    constexpr int RP = RPT / 2;
+    float2 Wx[RP], Wy[RP], NWy[RP], Sx[RP], Sy[RP];
+    {
+      const float2 gl = gs[(Nt - 1) * Q + b];
 #pragma unroll
-    for (int jr = 0; jr < RPT; ++jr) {
-      w[jr] = cmul(w0, pw[jr]);
-      S[jr] = gs[(Nt - 1) * Q + b];
+      for (int u = 0; u < RP; ++u) {
+        const float2 wa = cmul(w0, pw[2 * u]), wc = cmul(w0, pw[2 * u + 1]);
+        Wx[u] = make_float2(wa.x, wc.x);
+        Wy[u] = make_float2(wa.y, wc.y);
+        NWy[u] = pk_neg(Wy[u]);
+        Sx[u] = make_float2(gl.x, gl.x);
+        Sy[u] = make_float2(gl.y, gl.y);
+      }
     }
     for (int t = Nt - 2; t >= 0; --t) {
       const float2 gt = gs[t * Q + b];
+      const float2 gx = make_float2(gt.x, gt.x), gy = make_float2(gt.y, gt.y);
 #pragma unroll
-      for (int jr = 0; jr < RPT; ++jr)
-        S[jr] = make_float2(fmaf(S[jr].x, w[jr].x, fmaf(-S[jr].y, w[jr].y, gt.x)),
-                            fmaf(S[jr].x, w[jr].y, fmaf(S[jr].y, w[jr].x, gt.y)));
+      for (int u = 0; u < RP; ++u) {
+        const float2 tx = pk_fma(Sx[u], Wx[u], pk_fma(Sy[u], NWy[u], gx));
+        const float2 ty = pk_fma(Sx[u], Wy[u], pk_fma(Sy[u], Wx[u], gy));
+        Sx[u] = tx;
+        Sy[u] = ty;
+      }
+    }
+    float2 S[RPT];
+#pragma unroll
+    for (int u = 0; u < RP; ++u) {
+      S[2 * u] = make_float2(Sx[u].x, Sy[u].x);
+      S[2 * u + 1] = make_float2(Sx[u].y, Sy[u].y);
     }
     __syncthreads();  // buf is free
 #pragma unroll
