@@ -22,7 +22,7 @@ from .intfdr import intshift, intshift_, intfdr, intfdr_
 from .fftfdr import (FFTFDRWorkspace, fftfdr_workspace, fftfdr_workspace_, fdshiftsum,
                      fdshiftsum_, fdshift, fdshift_, fftfdr, fftfdr_)
 from .fdrutils import (create_fdr, fdrstats, fdrnormalize, fdrnormalize_, fdrdenormalize,
-                       fdrsynchronize, findprotohits)
+                       fdrsynchronize, findprotohits, cluster_protohits)
 
 _lib.load()  # fail loudly at import when the CUDA library is missing
 
@@ -36,5 +36,5 @@ __all__ = [
     "FFTFDRWorkspace", "fftfdr_workspace", "fftfdr_workspace_", "fdshiftsum", "fdshiftsum_",
     "fdshift", "fdshift_", "fftfdr", "fftfdr_",
     "create_fdr", "fdrstats", "fdrnormalize", "fdrnormalize_", "fdrdenormalize",
-    "fdrsynchronize", "findprotohits",
+    "fdrsynchronize", "findprotohits", "cluster_protohits",
 ]

@@ -54,6 +54,13 @@ class fdr_zdt_info(C.Structure):
     ]
 
 
+class fdr_hit_cluster(C.Structure):
+    _fields_ = [("peak_i", C.c_int64), ("peak_j", C.c_int64), ("peak_value", C.c_float),
+                ("reserved", C.c_int32), ("count", C.c_int64), ("i_min", C.c_int64),
+                ("i_max", C.c_int64), ("j_min", C.c_int64), ("j_max", C.c_int64),
+                ("first", C.c_int64)]
+
+
 class fdr_batch_channel(C.Structure):
     _fields_ = [("Nf", C.c_int64), ("Nt", C.c_int64), ("Nr", C.c_int64), ("r0", C.c_float),
                 ("dr", C.c_float), ("spectrogram", C.c_void_p), ("fdr", C.c_void_p)]
@@ -127,6 +134,8 @@ SIGNATURES = {
     "fdr_normalize": (INT, [C.POINTER(P), I64, I64, I64, F32, F32, P]),
     "fdr_findprotohits": (INT, [C.POINTER(P), I64, I64, I64, F64, INT, P, I64,
                                 C.POINTER(I64), C.POINTER(F64), P]),
+    "fdr_cluster_protohits": (INT, [P, I64, I64, I64, INT, INT, C.POINTER(P), I64, I64, P, P,
+                                    I64, C.POINTER(I64), P]),
 }
 
 _lib = None

@@ -93,3 +93,39 @@ def findprotohits(fdr, threshold, snr=False, capacity=None, stream=None, return_
         break
     out = hits[: count.value].cpu().numpy()
     return (out, thr.value) if return_threshold else out
+
+
+CLUSTER_DTYPE = np.dtype([("peak_i", "<i8"), ("peak_j", "<i8"), ("peak_value", "<f4"),
+                          ("reserved", "<i4"), ("count", "<i8"), ("i_min", "<i8"), ("i_max", "<i8"),
+                          ("j_min", "<i8"), ("j_max", "<i8"), ("first", "<i8")])
+
+
+def cluster_protohits(hits, Nf, Nj, di=1, dj=1, fdr=None, capacity=None, stream=None):
+    """Clusters of proto-hits (fdr_cluster_protohits): the connected components of ``hits``
+    (zero-based (i, j) pairs in the column-major order findprotohits returns, numpy or a
+    CUDA int64 tensor) where proto-hits within di channels and dj drift-rate columns touch.
+    ``fdr`` (one matrix or a list of rate batches covering the Nj columns) supplies the peak
+    values.  Returns (labels, clusters): per-hit cluster numbers (numpy int64) and a numpy
+    structured array with peak_i, peak_j, peak_value, count, i_min, i_max, j_min, j_max,
+    first, ordered by each cluster's first proto-hit."""
+    if isinstance(hits, torch.Tensor):
+        h = hits.to(device="cuda", dtype=torch.int64).reshape(-1, 2).contiguous()
+    else:
+        h = torch.from_numpy(np.ascontiguousarray(np.asarray(hits, dtype=np.int64).reshape(-1, 2))).cuda()
+    n = h.shape[0]
+    if n == 0:
+        return np.zeros(0, np.int64), np.zeros(0, CLUSTER_DTYPE)
+    if fdr is not None:
+        mats, _ = _mats(fdr)
+        arr, nb, Nrb = _ptr_array(mats), len(mats), mats[0].shape[1]
+    else:
+        arr, nb, Nrb = None, 0, 0
+    labels = torch.empty(n, dtype=torch.int64, device="cuda")
+    cap = n if capacity is None else int(capacity)
+    out = torch.empty((max(1, cap), CLUSTER_DTYPE.itemsize), dtype=torch.uint8, device="cuda")
+    count = C.c_int64()
+    _lib.check(_lib.lib().fdr_cluster_protohits(ptr(h), n, int(Nf), int(Nj), int(di), int(dj), arr,
+                                                nb, Nrb, ptr(labels), ptr(out), cap, C.byref(count),
+                                                stream_handle(stream)))
+    clusters = np.frombuffer(out[: count.value].cpu().numpy().tobytes(), dtype=CLUSTER_DTYPE)
+    return labels.cpu().numpy(), clusters

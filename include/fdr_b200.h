@@ -328,6 +328,34 @@ int fdr_findprotohits(const float* const* fdrs, int64_t nb, int64_t Nf, int64_t 
                       double threshold, int snr, int64_t* hits, int64_t capacity,
                       int64_t* count, double* threshold_used, fdr_stream_t stream);
 
+/* ---------------------------------------------------------------------------------- */
+/* Proto-hits -> hits.  No counterpart in the reference: it is the step after           */
+/* findprotohits that README.md:57-66 places in DopplerDriftSearchTools.jl.             */
+/* ---------------------------------------------------------------------------------- */
+typedef struct fdr_hit_cluster {
+  int64_t peak_i, peak_j; /* zero-based cell of the largest FDR value (first in column-major
+                             order on ties; the first hit when no FDR is given) */
+  float peak_value;       /* FDR value there (NaN when no FDR is given) */
+  int32_t reserved;
+  int64_t count;          /* proto-hits in the cluster */
+  int64_t i_min, i_max, j_min, j_max; /* bounding box */
+  int64_t first;          /* index into the hit list of the cluster's first hit */
+} fdr_hit_cluster;
+
+/* Connected components of the proto-hits `hits` (device, nhits (i, j) int64 pairs in the
+   column-major order findprotohits returns; i < Nf, j < Nj) where two proto-hits touch
+   when |i - i'| <= di and |j - j'| <= dj (no wrap-around).  Clusters are numbered in the
+   order of their first proto-hit; labels (device, nhits int64, may be NULL) receive each
+   proto-hit's cluster; clusters (device, capacity entries) their summaries, with peak
+   values read from the FDR matrices fdrs[0..nb) of Nrb columns each (host array of device
+   pointers, nb*Nrb == Nj; may be NULL).  Synchronises `stream`; *nclusters (host) receives
+   the number of clusters; more than `capacity` returns FDR_ERR_CAPACITY (labels are still
+   complete).  Unsorted or out-of-range hits return FDR_ERR_INVALID_ARGUMENT. */
+int fdr_cluster_protohits(const int64_t* hits, int64_t nhits, int64_t Nf, int64_t Nj, int di,
+                          int dj, const float* const* fdrs, int64_t nb, int64_t Nrb,
+                          int64_t* labels, fdr_hit_cluster* clusters, int64_t capacity,
+                          int64_t* nclusters, fdr_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -652,3 +652,62 @@ def propose_lag_features(spec, factor=256, maxlag=8, compress=False):
         prod = (s[:, :-1] * np.roll(s[:, 1:], -l, axis=0)).sum(axis=1)
         out[li] = prod.reshape(Nf // factor, factor).sum(axis=1)
     return _compress(out / math.sqrt(factor * (Nt - 1)), compress)
+
+
+# ----------------------------------------------------------------------------------------
+# Proto-hits -> hits (connected components; the step after findprotohits)
+# ----------------------------------------------------------------------------------------
+
+def cluster_protohits(hits, Nf, di=1, dj=1, fdr=None):
+    """Union-find restatement of the device clustering: proto-hits (zero-based (i, j), in
+    column-major order) touch when |Δi| <= di and |Δj| <= dj (no wrap).  Returns
+    (labels, clusters): clusters numbered by their first proto-hit, each a dict with
+    count, i_min, i_max, j_min, j_max, first, peak_i, peak_j, peak_value (largest FDR value,
+    earliest proto-hit on ties; the first proto-hit and NaN without an FDR)."""
+    hits = np.asarray(hits, dtype=np.int64).reshape(-1, 2)
+    n = len(hits)
+    index = {(int(i), int(j)): h for h, (i, j) in enumerate(hits)}
+    parent = list(range(n))
+
+    def find(x):
+        while parent[x] != x:
+            parent[x] = parent[parent[x]]
+            x = parent[x]
+        return x
+
+    for h, (i, j) in enumerate(hits):
+        for dc in range(-dj, dj + 1):
+            for dr in range(-di, di + 1):
+                if not (0 <= int(i) + dr < Nf):
+                    continue
+                g = index.get((int(i) + dr, int(j) + dc))
+                if g is None:
+                    continue
+                a, b = find(h), find(g)
+                if a != b:
+                    parent[max(a, b)] = min(a, b)
+    roots = [find(h) for h in range(n)]
+    order = sorted(set(roots))
+    cid = {r: c for c, r in enumerate(order)}
+    labels = np.array([cid[r] for r in roots], dtype=np.int64)
+    mats = None
+    if fdr is not None:
+        mats = fdr if isinstance(fdr, (list, tuple)) else [fdr]
+    members_of = {r: [] for r in order}
+    for h, r in enumerate(roots):
+        members_of[r].append(h)
+    clusters = []
+    for r in order:
+        members = members_of[r]
+        ii, jj = hits[members, 0], hits[members, 1]
+        if mats is not None:
+            Nrb = mats[0].shape[1]
+            vals = [np.float32(mats[int(j) // Nrb][int(i), int(j) % Nrb]) for i, j in zip(ii, jj)]
+            best = max(range(len(members)), key=lambda m: (vals[m], -members[m]))
+            pv = float(vals[best])
+        else:
+            best, pv = 0, float("nan")
+        clusters.append({"count": len(members), "i_min": int(ii.min()), "i_max": int(ii.max()),
+                         "j_min": int(jj.min()), "j_max": int(jj.max()), "first": int(r),
+                         "peak_i": int(ii[best]), "peak_j": int(jj[best]), "peak_value": pv})
+    return labels, clusters

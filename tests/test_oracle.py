@@ -160,3 +160,15 @@ def test_proposal_features_restatement(oracle):
     ref = sum((s[n, t] - 1) * (s[(n + l) % Nf, t + 1] - 1)
               for n in range(512, 768) for t in range(Nt - 1)) / np.sqrt(256 * (Nt - 1))
     assert np.isclose(lf[l + 8, b], ref)
+
+
+def test_cluster_restatement_small(oracle):
+    """Hand-checked components of the clustering restatement."""
+    hits = np.array([[1, 0], [2, 0], [7, 0], [3, 1], [8, 2], [0, 4]])
+    labels, cl = oracle.cluster_protohits(hits, 10, 1, 1)
+    # (1,0)-(2,0)-(3,1) touch; (7,0) alone ((8,2) is two columns away); (8,2); (0,4)
+    assert list(labels) == [0, 0, 1, 0, 2, 3]
+    assert [c["count"] for c in cl] == [3, 1, 1, 1]
+    assert cl[0]["i_max"] == 3 and cl[0]["j_max"] == 1 and cl[0]["first"] == 0
+    labels2, _ = oracle.cluster_protohits(hits, 10, 1, 2)
+    assert labels2[2] == labels2[4]  # (7,0)-(8,2) with dj = 2
