@@ -122,6 +122,7 @@ SIGNATURES = {
     "fdr_intshift": (INT, [P, I64, I64, F64, INT, P, P]),
     "fdr_intfdr": (INT, [P, I64, I64, C.POINTER(F64), I64, INT, P, P]),
     "fdr_intfdr_shifts": (INT, [P, I64, I64, C.POINTER(I64), I64, P, P]),
+    "fdr_taylor_tree": (INT, [P, I64, I64, INT, INT, P, P]),
     "fdr_fftfdr_workspace": (INT, [C.POINTER(P), P, I64, I64, P]),
     "fdr_fftfdr_workspace_update": (INT, [P, P, I64, I64, P]),
     "fdr_fftfdr_destroy": (INT, [P]),

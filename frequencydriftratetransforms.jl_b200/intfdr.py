@@ -83,3 +83,44 @@ def intfdr(spectrogram, rates, stream=None):
     Nr = len(rates)
     fdr = fortran_empty(spec.shape[0], Nr)
     return intfdr_(fdr, spec, rates, stream)
+
+
+def taylor_shifts(Nt, d):
+    """Channel offsets p_d(t), t < Nt, of the Taylor-tree path of total drift d (Nt a power of
+    two): the path of drift floor(|d|/2) over each half, the second half offset by
+    ceil(|d|/2), negated for d < 0."""
+    if Nt & (Nt - 1) or Nt < 1 or abs(d) > max(Nt - 1, 0):
+        raise ValueError("Nt must be a power of two and |d| <= Nt-1")
+
+    def path(L, dd):
+        if L == 1:
+            return [0]
+        half = path(L // 2, dd // 2)
+        return half + [(dd + 1) // 2 + x for x in half]
+
+    p = path(Nt, abs(d))
+    return [x if d >= 0 else -x for x in p]
+
+
+def taylorfdr_(fdr, spectrogram, dmin, dmax, stream=None):
+    """Taylor-tree integer FDR (fdr_taylor_tree) into ``fdr`` (Nf, dmax-dmin+1): column
+    d - dmin sums the spectrogram along the tree path of total drift d, i.e. approximately
+    intfdr at rate d/(Nt-1) (exactly for d = 0 and |d| = Nt-1; taylor_shifts gives the
+    paths)."""
+    spec = as_device_f32(spectrogram)
+    Nf, Nt = spec.shape
+    if tuple(fdr.shape) != (Nf, dmax - dmin + 1):
+        raise _lib.FDRError(_lib.FDR_ERR_INVALID_ARGUMENT, "fdr has the wrong size")
+    _lib.check(_lib.lib().fdr_taylor_tree(ptr(spec), Nf, Nt, int(dmin), int(dmax), ptr(fdr),
+                                          stream_handle(stream)))
+    return fdr
+
+
+def taylorfdr(spectrogram, dmin=None, dmax=None, stream=None):
+    """Allocating form of taylorfdr_; the drifts default to -(Nt-1)..Nt-1."""
+    spec = as_device_f32(spectrogram)
+    Nt = spec.shape[1]
+    dmin = -(Nt - 1) if dmin is None else dmin
+    dmax = Nt - 1 if dmax is None else dmax
+    fdr = fortran_empty(spec.shape[0], dmax - dmin + 1)
+    return taylorfdr_(fdr, spec, dmin, dmax, stream)

@@ -263,6 +263,16 @@ int fdr_intfdr(const float* spec, int64_t Nf, int64_t Nt, const double* rates, i
    (shift of rate j at time t at shifts[j*Nt + t]). */
 int fdr_intfdr_shifts(const float* spec, int64_t Nf, int64_t Nt, const int64_t* shifts,
                       int64_t Nr, float* fdr, fdr_stream_t stream);
+/* Taylor-tree integer FDR (the faster intfdr variant README.md:88-92 mentions; no
+   counterpart in the reference code).  Nt a power of two in [2, 64]; column d - dmin of
+   fdr (device, Nf x (dmax-dmin+1) column-major) for each integer total drift d in
+   [dmin, dmax] (|d| <= Nt-1, rate d/(Nt-1) channels per step) sums
+   spec[(n + p_d(t)) mod Nf, t] along the tree path p_d: p_d = 0 for Nt = 1, and over 2L
+   steps the path of drift floor(|d|/2) over the first L steps followed by the same path
+   over the last L steps offset by ceil(|d|/2) (negated for d < 0).  d = 0 and |d| = Nt-1
+   equal intfdr at rates 0 and +-1; float32 pairwise additions in a fixed order. */
+int fdr_taylor_tree(const float* spectrogram, int64_t Nf, int64_t Nt, int dmin, int dmax,
+                    float* fdr, fdr_stream_t stream);
 
 /* ---------------------------------------------------------------------------------- */
 /* fftfdr.jl                                                                           */

@@ -711,3 +711,34 @@ def cluster_protohits(hits, Nf, di=1, dj=1, fdr=None):
                          "j_min": int(jj.min()), "j_max": int(jj.max()), "first": int(r),
                          "peak_i": int(ii[best]), "peak_j": int(jj[best]), "peak_value": pv})
     return labels, clusters
+
+
+# ----------------------------------------------------------------------------------------
+# Taylor tree (the faster integer FDR that README.md:88-92 mentions)
+# ----------------------------------------------------------------------------------------
+
+def taylor_tree(spec, dmin, dmax):
+    """Float32 restatement of the Taylor-tree FDR with the device's addition order: stage by
+    stage, row (block*2L + d) = row (2*block*L + d//2) + row ((2*block+1)*L + d//2) shifted by
+    ceil(d/2) channels (circularly; towards lower channels for the negative tree).  Returns
+    (Nf, dmax-dmin+1) float32, column d - dmin."""
+    s = np.asarray(spec, dtype=np.float32)
+    Nf, Nt = s.shape
+    assert Nt & (Nt - 1) == 0
+    out = np.empty((Nf, dmax - dmin + 1), dtype=np.float32)
+    for sgn in (+1, -1):
+        A = s.T.copy()  # rows = steps
+        L = 1
+        while L < Nt:
+            B = np.empty_like(A)
+            for blk in range(Nt // (2 * L)):
+                for d in range(2 * L):
+                    top = A[2 * blk * L + d // 2]
+                    bot = np.roll(A[(2 * blk + 1) * L + d // 2], -sgn * ((d + 1) // 2))
+                    B[blk * 2 * L + d] = top + bot
+            A = B
+            L *= 2
+        for d in range(dmin, dmax + 1):
+            if (d >= 0) == (sgn > 0):
+                out[:, d - dmin] = A[abs(d)]
+    return out

@@ -172,3 +172,21 @@ def test_cluster_restatement_small(oracle):
     assert cl[0]["i_max"] == 3 and cl[0]["j_max"] == 1 and cl[0]["first"] == 0
     labels2, _ = oracle.cluster_protohits(hits, 10, 1, 2)
     assert labels2[2] == labels2[4]  # (7,0)-(8,2) with dj = 2
+
+
+def test_taylor_restatement_is_a_path_sum(oracle, fdr):
+    """The float32 Taylor-tree restatement equals the sum along taylor_shifts' paths (integer
+    data: exact), the paths end at channel d and stay near the straight line."""
+    rng = np.random.default_rng(2)
+    Nf, Nt = 64, 16
+    s = rng.integers(0, 50, (Nf, Nt)).astype(np.float32)
+    out = oracle.taylor_tree(s, -(Nt - 1), Nt - 1)
+    idx = np.arange(Nf)
+    worst = 0.0
+    for d in range(-(Nt - 1), Nt):
+        p = fdr.taylor_shifts(Nt, d)
+        assert p[0] == 0 and p[-1] == d
+        ref = sum(s[(idx + p[t]) % Nf, t].astype(np.float64) for t in range(Nt))
+        assert np.array_equal(out[:, d + Nt - 1], ref.astype(np.float32))
+        worst = max(worst, max(abs(p[t] - d * t / (Nt - 1)) for t in range(Nt)))
+    assert worst <= 1.0  # within one channel of the straight line (0.67 at Nt = 16)
