@@ -94,6 +94,35 @@ def fp32_peak_tflops(torch):
         torch.backends.cuda.matmul.allow_tf32 = prev
 
 
+def taylor_leg(fdr, torch, spec_dev, steps=20):
+    """Taylor-tree FDR against brute-force intfdr on the bench spectrogram (Nf=2^20, Nt=16)
+    at the 31 integer total drifts -15..15 (rates d/15 ch/step), device-timed."""
+    nd = 2 * NT - 1
+    out_t = fdr.fortran_empty(NF, nd)
+    out_i = fdr.fortran_empty(NF, nd)
+    rates = [d / (NT - 1) for d in range(-(NT - 1), NT)]
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        e1.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    t_tree = timed(lambda: fdr.taylorfdr_(out_t, spec_dev, -(NT - 1), NT - 1))
+    t_int = timed(lambda: fdr.intfdr_(out_i, spec_dev, rates))
+    cells = NF * nd
+    alg = 4 * NF * NT + 4 * NF * nd
+    return {"workload": "Nf=2^20 x Nt=16, 31 integer drifts -15..15", "taylor_ms": t_tree,
+            "taylor_cells_per_s": cells / (t_tree * 1e-3), "intfdr_ms": t_int,
+            "intfdr_cells_per_s": cells / (t_int * 1e-3),
+            "taylor_gbs_algorithmic": alg / (t_tree * 1e-3) / 1e9}
+
+
 def proposal_leg(fdr, torch, nchan=64):
     """Learned rate-window proposal on held-out synthetic channels (Nf=2^20, Nt=16, 0-5 tones
     of amplitude 8-40, rates in [-8, 8]): the trained network (power + lag input) at its
@@ -280,6 +309,8 @@ def main():
                     help="skip the batched multi-channel leg (64 uneven coarse channels)")
     ap.add_argument("--no-proposal", action="store_true",
                     help="skip the learned rate-window proposal leg")
+    ap.add_argument("--no-taylor", action="store_true",
+                    help="skip the Taylor-tree vs intfdr leg")
     ap.add_argument("--no-fp32-peak", action="store_true",
                     help="skip the SGEMM measurement of the FP32 peak (compute.frac)")
     args = ap.parse_args()
@@ -411,6 +442,7 @@ def main():
     batched = None
     if not args.no_batched:
         batched = batched_leg(fdr, torch, max(3, min(args.steps, 10)))
+    taylor = taylor_leg(fdr, torch, specs[0]) if rank == 0 and not args.no_taylor else None
     proposal = None
     if rank == 0 and not args.no_proposal:
         proposal = proposal_leg(fdr, torch)
@@ -455,6 +487,7 @@ def main():
             "cpu_baseline": cpu,
             "batched": batched,
             "proposal": proposal,
+            "taylor": taylor,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
