@@ -123,6 +123,40 @@ def taylor_leg(fdr, torch, spec_dev, steps=20):
             "taylor_gbs_algorithmic": alg / (t_tree * 1e-3) / 1e9}
 
 
+def ingest_leg(fdr, torch, host_specs):
+    """File-to-hits pipeline: a SIGPROC filterbank of len(host_specs) coarse channels (the
+    bench spectrograms side by side, Nf=2^20 fine channels each, Nt=16) in the page cache,
+    searched by SearchPipeline (gather into pinned memory, copy, zdtfdr! with the fused
+    findprotohits at SNR 10, proto-hit clustering), wall clock including everything."""
+    import tempfile
+    nco = len(host_specs)
+    data = np.empty((NT, 1, NF * nco), np.float32)
+    for c, h in enumerate(host_specs):
+        data[:, 0, c * NF:(c + 1) * NF] = h.T
+    fd, path = tempfile.mkstemp(suffix=".fil")
+    os.close(fd)
+    try:
+        fdr.write_filterbank(path, {"fch1": 8400.0, "foff": -2.79e-6, "tsamp": 18.25, "nbits": 32}, data)
+        del data
+        fb = fdr.Filterbank(path)
+        pipe = fdr.SearchPipeline(NF, NT, R0, DR, NR, snr=HIT_SNR)
+        pipe.run(fb)  # warm-up (and page cache)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        reps = 3
+        for _ in range(reps):
+            res = pipe.run(fb)
+        torch.cuda.synchronize()
+        dt = (time.perf_counter() - t0) / reps
+        nclu = sum(len(r[3]) for r in res)
+        nhits = sum(len(r[1]) for r in res)
+        return {"workload": f"filterbank file, {nco} coarse channels of 2^20 x 16, 129 rates",
+                "cells_per_s": NF * NR * nco / dt, "ms_per_coarse_channel": dt / nco * 1e3,
+                "protohits": nhits, "clusters": nclu}
+    finally:
+        os.remove(path)
+
+
 def proposal_leg(fdr, torch, nchan=64):
     """Learned rate-window proposal on held-out synthetic channels (Nf=2^20, Nt=16, 0-5 tones
     of amplitude 8-40, rates in [-8, 8]): the trained network (power + lag input) at its
@@ -309,6 +343,8 @@ def main():
                     help="skip the batched multi-channel leg (64 uneven coarse channels)")
     ap.add_argument("--no-proposal", action="store_true",
                     help="skip the learned rate-window proposal leg")
+    ap.add_argument("--no-ingest", action="store_true",
+                    help="skip the filterbank-file search pipeline leg")
     ap.add_argument("--no-taylor", action="store_true",
                     help="skip the Taylor-tree vs intfdr leg")
     ap.add_argument("--no-fp32-peak", action="store_true",
@@ -443,6 +479,7 @@ def main():
     if not args.no_batched:
         batched = batched_leg(fdr, torch, max(3, min(args.steps, 10)))
     taylor = taylor_leg(fdr, torch, specs[0]) if rank == 0 and not args.no_taylor else None
+    ingest = ingest_leg(fdr, torch, host_specs) if rank == 0 and not args.no_ingest else None
     proposal = None
     if rank == 0 and not args.no_proposal:
         proposal = proposal_leg(fdr, torch)
@@ -488,6 +525,7 @@ def main():
             "batched": batched,
             "proposal": proposal,
             "taylor": taylor,
+            "ingest": ingest,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
