@@ -11,14 +11,15 @@ a keyword header (HEADER_START ... HEADER_END) followed by time-major samples, e
 ``SearchPipeline`` runs zdtfdr! + findprotohits + proto-hit clustering over the coarse
 channels of a file: each coarse channel's spectrogram (Nf fine channels x Nt steps, Julia
 column-major layout, which is exactly the time-major file layout of that channel range) is
-gathered into one of two pinned host buffers, copied to the device on a copy stream, and
-searched on the compute stream while the next channel is gathered and copied.
+gathered by a pool of host threads into one of two pinned host buffers, copied to the
+device on a copy stream, and searched on the compute stream while the next channel is
+gathered.
 """
 from __future__ import annotations
 
 import os
 import struct
-import time
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 import torch
@@ -137,6 +138,9 @@ class SearchPipeline:
         self.pinned = [torch.empty(nfpc * nt, dtype=torch.float32).pin_memory() for _ in range(2)]
         self.dev = [torch.empty(nfpc * nt, dtype=torch.float32, device="cuda") for _ in range(2)]
         self.copy_stream = torch.cuda.Stream()
+        self.ready = [torch.cuda.Event(), torch.cuda.Event()]
+        self.nthreads = max(1, min(8, os.cpu_count() or 1))
+        self.pool = ThreadPoolExecutor(max_workers=self.nthreads)
         self.r0, self.dr, self.Nr = r0, dr, Nr
 
     def _spec_view(self, k):
@@ -148,39 +152,49 @@ class SearchPipeline:
         labels, clusters = cluster_protohits(hits, self.nfpc, self.Nr, self.di, self.dj, fdr=self.dest)
         return hits, labels, clusters
 
+    def _gather(self, fb, c, k, ifno, t0):
+        """Copy coarse channel c into pinned buffer k, the time steps split over the pool."""
+        out = self.pinned[k].numpy().reshape(self.nt, self.nfpc)
+        lo, hi = c * self.nfpc, (c + 1) * self.nfpc
+        step = max(1, self.nt // self.nthreads)
+
+        def rows(a, b):
+            out[a:b] = fb.data[t0 + a:t0 + b, ifno, lo:hi]
+
+        return [self.pool.submit(rows, a, min(self.nt, a + step)) for a in range(0, self.nt, step)]
+
+    def _copy(self, k, futures):
+        for f in futures:
+            f.result()
+        with torch.cuda.stream(self.copy_stream):
+            self.dev[k].copy_(self.pinned[k], non_blocking=True)
+            self.ready[k].record(self.copy_stream)
+
     def run(self, fb, channels=None, ifno=0, t0=0):
         """Search the coarse channels ``channels`` (default: all) of Filterbank ``fb``;
-        returns a list of (channel, hits, labels, clusters)."""
+        returns a list of (channel, hits, labels, clusters).  While channel i is searched,
+        host threads gather channel i+1 into the other pinned buffer; its copy to the
+        device is issued as soon as the gather is done."""
         nco = fb.nchans // self.nfpc
         channels = list(range(nco)) if channels is None else list(channels)
+        if fb.nsamples - t0 < self.nt:
+            raise ValueError("the file holds fewer time steps than the pipeline's Nt")
         results = []
         cur = torch.cuda.current_stream()
-        ready = [torch.cuda.Event(), torch.cuda.Event()]
-        free = [torch.cuda.Event(), torch.cuda.Event()]
-        for e in free:
-            e.record(cur)
-
-        def stage(i):
-            k = i % 2
-            c = channels[i]
-            free[k].synchronize()  # the previous search on this buffer has consumed it
-            fb.spectrogram(c * self.nfpc, (c + 1) * self.nfpc, ifno, t0, self.nt,
-                           out=self.pinned[k].numpy())
-            with torch.cuda.stream(self.copy_stream):
-                self.copy_stream.wait_event(free[k])
-                self.dev[k].copy_(self.pinned[k], non_blocking=True)
-                ready[k].record(self.copy_stream)
-
         if channels:
-            stage(0)
+            self._copy(0, self._gather(fb, channels[0], 0, ifno, t0))
         for i, c in enumerate(channels):
             k = i % 2
+            nxt = None
             if i + 1 < len(channels):
-                stage(i + 1)
-            cur.wait_event(ready[k])
+                # buffer 1-k was last used by channel i-1, whose search has returned (it
+                # synchronises), so both its pinned and its device copy are free
+                nxt = self._gather(fb, channels[i + 1], 1 - k, ifno, t0)
+            cur.wait_event(self.ready[k])
             hits, labels, clusters = self.search_channel(self._spec_view(k))
-            free[k].record(cur)
             results.append((c, hits, labels, clusters))
+            if nxt is not None:
+                self._copy(1 - k, nxt)
         return results
 
     def hit_table(self, fb, results):
