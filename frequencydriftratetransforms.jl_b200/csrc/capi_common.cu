@@ -7,6 +7,7 @@
 #include <mutex>
 
 #include "fdr_internal.cuh"
+#include "zdt_ws.cuh"
 
 namespace fdr {
 
@@ -147,7 +148,7 @@ int fdr_synchronize(fdr_stream_t stream) {
   } else {
     FDR_CUDA(cudaDeviceSynchronize());
   }
-  return FDR_OK;
+  return fdr::fused_take_fault();
 }
 
 int64_t fdr_calc_nl(int64_t Nt, int64_t Nr, const int64_t* factors, int nfactors) {

@@ -25,6 +25,8 @@
 // hence dyadic, so k*r_j/Nf is an exact fraction m / 2^bits with m computed in 64-bit
 // integer arithmetic modulo 2^bits; only the final conversion to a float in [-1, 1)
 // half-turns rounds.
+#include <cuda.h>  // CUtensorMap (the encode entry point is fetched from the runtime)
+#include <cudaTypedefs.h>
 #include <math.h>
 #include <string.h>
 
@@ -811,6 +813,189 @@ zdtf_output2_kernel(const float2* __restrict__ W, long long N, int Q, int Nr,
 }
 
 // ------------------------------------------------------------------------------------
+// Output pass with TMA (P = P1*P2 <= 1024 split as in zdtf_output2_kernel): a persistent
+// grid, one CTA per SM, walks the (rate pair, 8-residue) tiles; the W tile of the next-but-one
+// tile is fetched by the tensor-memory accelerator into the other half of a double buffer
+// (4 boxes of 256 k1 rows x 8 complex, 64 KB) while the current tile is transformed, so the
+// HBM reads overlap the DFTs and the FDR stores.  Waits on the mbarriers are bounded by
+// kTmaWaitNs of %globaltimer; a wait that runs out sets g_fused_fault and the CTA returns
+// after a bounded wait for its copies in flight (reported by fdr_synchronize).
+// ------------------------------------------------------------------------------------
+__device__ int g_fused_fault;
+constexpr unsigned long long kTmaWaitNs = 1000000000ull;  // 1 s
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
+  const unsigned long long t0 = global_ns();
+  while (!mbar_try_wait(bar, parity))
+    if (global_ns() - t0 > kTmaWaitNs) return false;
+  return true;
+}
+// 2-D tiled TMA load (no multicast) of box {x .. x+15 floats, y .. y+255 rows} into dst.
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y,
+                                            unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+      ::"r"(smem_addr(dst)), "l"((unsigned long long)map), "r"(x), "r"(y), "r"(smem_addr(bar))
+      : "memory");
+}
+
+template <int P1, int P2, int TS>
+struct OutTmaShape {
+  static constexpr int P = P1 * P2;
+  static constexpr int T = TS * (P1 > P2 ? P1 : P2);
+  static constexpr int S1 = P2 + 1;
+  static constexpr int SSEQ = ((P1 * S1 + 15) / 16) * 16 + 2;
+  static constexpr int BOXR = 256;                 // k1 rows per TMA box
+  static constexpr int NBOX = P / BOXR;
+  static constexpr unsigned STAGE = sizeof(float2) * P * TS;  // bytes of one W tile
+  static constexpr size_t SMEM = 1024 + 2 * (size_t)STAGE + sizeof(float2) * (TS * SSEQ + P) + 16;
+  static_assert(P % BOXR == 0 && TS * 2 * sizeof(float) % 16 == 0, "TMA box shape");
+};
+
+template <int P1, int P2, int TS>
+__global__ void __launch_bounds__(OutTmaShape<P1, P2, TS>::T, 1)
+zdtf_output_tma_kernel(const __grid_constant__ CUtensorMap wmap, long long N, int Q, int Nr,
+                       int npairs, float* __restrict__ dest, const float2* __restrict__ rootsP,
+                       double* __restrict__ acc) {
+  using SH = OutTmaShape<P1, P2, TS>;
+  constexpr int P = SH::P, S1 = SH::S1, SSEQ = SH::SSEQ;
+  extern __shared__ unsigned char smraw[];
+  const uintptr_t base = ((uintptr_t)smraw + 1023) & ~(uintptr_t)1023;
+  float2* stage0 = (float2*)base;
+  float2* stage1 = (float2*)(base + SH::STAGE);
+  float2* buf = (float2*)(base + 2 * (size_t)SH::STAGE);
+  float2* roots = buf + TS * SSEQ;  // exp(-2 pi i m / P)
+  unsigned long long* bar = (unsigned long long*)(roots + P);
+  const int tid = threadIdx.x;
+  const int ntna = Q / TS;
+  const long long ntiles = (long long)ntna * npairs;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  for (int i = tid; i < P; i += SH::T) roots[i] = __ldg(rootsP + i);
+  __syncthreads();
+  auto issue = [&](long long tile, int st) {  // thread 0 only
+    const int q = (int)(tile / ntna), nat = (int)(tile - (long long)q * ntna);
+    float2* dst = st ? stage1 : stage0;
+    mbar_expect_tx(&bar[st], SH::STAGE);
+#pragma unroll
+    for (int b = 0; b < SH::NBOX; ++b)
+      tma_load_2d(dst + b * SH::BOXR * TS, &wmap, 2 * TS * nat, q * P + b * SH::BOXR, &bar[st]);
+  };
+  const long long first = blockIdx.x, stride = gridDim.x;
+  if (tid == 0) {
+    if (first < ntiles) issue(first, 0);
+    if (first + stride < ntiles) issue(first + stride, 1);
+  }
+  const int seq = tid % TS;
+  const int r = tid / TS;  // k1a in pass 1, nb_b in pass 2
+  int it = 0;
+  for (long long tile = first; tile < ntiles; tile += stride, ++it) {
+    const int st = it & 1;
+    const unsigned parity = (unsigned)((it >> 1) & 1);
+    const bool ok = mbar_wait_bounded(&bar[st], parity);
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) {
+        atomicOr(&g_fused_fault, 1);
+        // the other buffer's copy, if one was issued, before the shared memory goes away
+        if (tile + stride < ntiles) (void)mbar_wait_bounded(&bar[st ^ 1], (unsigned)(((it + 1) >> 1) & 1));
+      }
+      return;
+    }
+    const float2* stg = st ? stage1 : stage0;
+    const int q = (int)(tile / ntna), nat = (int)(tile - (long long)q * ntna);
+    const int na0 = nat * TS;
+    float2 v[P2];
+    if (r < P1) {
+#pragma unroll
+      for (int m = 0; m < P2; ++m) v[m] = stg[(r + P1 * m) * TS + seq];
+    }
+    __syncthreads();  // this buffer is read: refill it with the next-but-one tile
+    if (tid == 0 && tile + 2 * stride < ntiles) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      issue(tile + 2 * stride, st);
+    }
+    if (r < P1) {
+      Dft<P2>::run(v, +1);
+      float2* b = buf + seq * SSEQ + r * S1;
+#pragma unroll
+      for (int nbb = 0; nbb < P2; ++nbb) {
+        const float2 t = roots[(r * nbb) & (P - 1)];
+        b[nbb] = cmul(v[nbb], make_float2(t.x, -t.y));
+      }
+    }
+    __syncthreads();
+    const int j = 2 * q;
+    const bool has1 = (j + 1) < Nr;
+    double m[4] = {0.0, 0.0, 0.0, 0.0};
+    if (r < P2) {
+      float2 w[P1];
+      const float2* b = buf + seq * SSEQ + r;
+#pragma unroll
+      for (int k1a = 0; k1a < P1; ++k1a) w[k1a] = b[k1a * S1];
+      Dft<P1>::run(w, +1);
+      float* d0 = dest + (long long)j * N + na0 + seq + (long long)Q * r;
+      float* d1 = d0 + N;
+#pragma unroll
+      for (int nba = 0; nba < P1; ++nba) {
+        const long long off = (long long)Q * P2 * nba;
+        __stcs(d0 + off, w[nba].x);
+        if (has1) __stcs(d1 + off, w[nba].y);
+      }
+      if (acc) {
+#pragma unroll
+        for (int nba = 0; nba < P1; ++nba) {
+          const double x = w[nba].x, y = has1 ? w[nba].y : 0.f;
+          m[0] += x; m[1] += x * x; m[2] += y; m[3] += y * y;
+        }
+      }
+    }
+    if (acc) {  // block reduction of the column moments, then one atomic add per value
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        for (int o = 16; o > 0; o >>= 1) m[i] += __shfl_down_sync(0xffffffffu, m[i], o);
+      __shared__ double red[4][SH::T / 32];
+      const int wid = tid >> 5;
+      if ((tid & 31) == 0)
+        for (int i = 0; i < 4; ++i) red[i][wid] = m[i];
+      __syncthreads();
+      if (tid < 4) {
+        double t = 0.0;
+        for (int i = 0; i < SH::T / 32; ++i) t += red[tid][i];
+        if (tid < 2 || has1) atomicAdd(acc + 2 * j + tid, t);
+      }
+    }
+    __syncthreads();  // buf (and red) are free for the next tile
+  }
+}
+
+// ------------------------------------------------------------------------------------
 // Host side
 // ------------------------------------------------------------------------------------
 // Tile (sequences per CTA) and block size of kernels A and C for a given P: one radix-16
@@ -942,6 +1127,9 @@ static int set_smem_attrs() {
                                 (int)Out2Shape<P1, P2, 8>::SMEM));
   SET_C2(8, 8) SET_C2(8, 16) SET_C2(16, 16) SET_C2(16, 32) SET_C2(32, 32)
 #undef SET_C2
+  FDR_CUDA(cudaFuncSetAttribute(zdtf_output_tma_kernel<32, 32, 8>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)OutTmaShape<32, 32, 8>::SMEM));
 #define SET_B(Q)                                                                               \
   FDR_CUDA(cudaFuncSetAttribute(zdtf_czt_kernel<Q, kFusedMaxNt>,                               \
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CztShape<Q>::SMEM)); \
@@ -1141,8 +1329,71 @@ int fused_czt_blocks(const FusedPlan* st, const float2* A, float2* W, float r0, 
   return FDR_ERR_UNSUPPORTED_SIZE;
 }
 
+// cuTensorMapEncodeTiled from the driver, through the runtime (no link against libcuda).
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+            cudaSuccess && q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    else
+      (void)cudaGetLastError();
+  }
+  return fn;
+}
+
+// Tensor map of W as a 2-D float32 array: rows (rate pair, k1) of 2*Q floats, 16 x 256 boxes.
+static bool w_tensor_map(CUtensorMap* map, const float2* W, int64_t Q, int64_t rows, int ts) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc || ((uintptr_t)W & 15) != 0) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)(2 * Q), (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)(2 * Q * sizeof(float))};
+  const cuuint32_t box[2] = {(cuuint32_t)(2 * ts), 256u};
+  const cuuint32_t estr[2] = {1u, 1u};
+  return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void*)W, dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// FDR_NO_TMA=1 in the environment selects the register-load output kernel instead.
+static bool tma_output_enabled() {
+  const char* e = getenv("FDR_NO_TMA");
+  return !(e && e[0] == '1');
+}
+
+int fused_take_fault() {
+  int h = 0;
+  if (cudaMemcpyFromSymbol(&h, g_fused_fault, sizeof(int)) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return FDR_OK;
+  }
+  if (h) {
+    const int z = 0;
+    (void)cudaMemcpyToSymbol(g_fused_fault, &z, sizeof(int));
+    set_error(FDR_ERR_CUDA, "fused output: a TMA wait timed out (the FDR is incomplete)");
+    return FDR_ERR_CUDA;
+  }
+  return FDR_OK;
+}
+
 int fused_output(const FusedPlan* st, const float2* W, float* dest, double* acc, cudaStream_t s) {
   const int P = st->P, Q = st->Q;
+  if (P == 1024 && Q >= 8 && tma_output_enabled()) {
+    CUtensorMap map;
+    if (w_tensor_map(&map, W, Q, st->npairs * (int64_t)P, 8)) {
+      using SH = OutTmaShape<32, 32, 8>;
+      const long long ntiles = (long long)(Q / 8) * st->npairs;
+      const int grid = (int)std::min<long long>(ntiles, sm_count());
+      zdtf_output_tma_kernel<32, 32, 8><<<grid, SH::T, SH::SMEM, s>>>(
+          map, st->N, Q, (int)st->Nr, (int)st->npairs, dest, st->tab.rootsP, acc);
+      FDR_LAUNCH_CHECK("zdtf_output_tma_kernel");
+      return FDR_OK;
+    }
+  }
 #define LAUNCH_C2(PP, P1, P2)                                                                  \
   if (P == PP) {                                                                               \
     using SH = Out2Shape<P1, P2, 8>;                                                           \

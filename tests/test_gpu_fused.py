@@ -153,3 +153,23 @@ def test_rate_blocks_argument_errors(fdr, oracle):
     st = fdr.ZDTWorkspace(spec, -2.0, 0.25, 16, staged_only=True)
     with pytest.raises(fdr.FDRError):
         fdr.zdtfdr_blocks_(fdr.fortran_empty(4096, 8), st, spec, [0])
+
+
+def test_tma_output_matches_register_output(fdr, oracle, monkeypatch):
+    """The output pass with TMA-fed double buffering (P = 1024) writes the same FDR, bit for
+    bit, as the register-load output kernel (FDR_NO_TMA=1), with and without the fused
+    proto-hit statistics, and reports no fault."""
+    for Nf, Nt, Nr in ((1 << 20, 16, 129), (1 << 18, 40, 33)):
+        spec = _spec(oracle, Nf, Nt, seed=Nf + Nt + 5)
+        ws = fdr.ZDTWorkspace(spec, -4.0, 1 / 16, Nr)
+        a = fdr.zdtfdr(ws).cpu().numpy()
+        ha, ta = fdr.zdtfdr_protohits_(fdr.fortran_empty(Nf, Nr), ws, spec, threshold=8.0,
+                                       return_threshold=True)
+        fdr.fdrsynchronize()
+        monkeypatch.setenv("FDR_NO_TMA", "1")
+        b = fdr.zdtfdr(ws).cpu().numpy()
+        hb, tb = fdr.zdtfdr_protohits_(fdr.fortran_empty(Nf, Nr), ws, spec, threshold=8.0,
+                                       return_threshold=True)
+        monkeypatch.delenv("FDR_NO_TMA")
+        assert np.array_equal(a, b)
+        assert ta == tb and np.array_equal(ha, hb)
