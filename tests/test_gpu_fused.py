@@ -158,8 +158,8 @@ def test_rate_blocks_argument_errors(fdr, oracle):
 def test_tma_output_matches_register_output(fdr, oracle, monkeypatch):
     """The output pass with TMA-fed double buffering (P = 1024) writes the same FDR, bit for
     bit, as the register-load output kernel (FDR_NO_TMA=1), with and without the fused
-    proto-hit statistics, and reports no fault."""
-    for Nf, Nt, Nr in ((1 << 20, 16, 129), (1 << 18, 40, 33)):
+    proto-hit statistics (odd Nt too), and reports no fault."""
+    for Nf, Nt, Nr in ((1 << 20, 16, 129), (1 << 18, 40, 33), (1 << 20, 15, 9)):
         spec = _spec(oracle, Nf, Nt, seed=Nf + Nt + 5)
         ws = fdr.ZDTWorkspace(spec, -4.0, 1 / 16, Nr)
         a = fdr.zdtfdr(ws).cpu().numpy()
