@@ -813,13 +813,12 @@ zdtf_output2_kernel(const float2* __restrict__ W, long long N, int Q, int Nr,
 }
 
 // ------------------------------------------------------------------------------------
-// Output pass with TMA (P = P1*P2 <= 1024 split as in zdtf_output2_kernel): a persistent
-// grid, one CTA per SM, walks the (rate pair, 8-residue) tiles; the W tile of the next-but-one
-// tile is fetched by the tensor-memory accelerator into the other half of a double buffer
-// (4 boxes of 256 k1 rows x 8 complex, 64 KB) while the current tile is transformed, so the
-// HBM reads overlap the DFTs and the FDR stores.  Waits on the mbarriers are bounded by
-// kTmaWaitNs of %globaltimer; a wait that runs out sets g_fused_fault and the CTA returns
-// after a bounded wait for its copies in flight (reported by fdr_synchronize).
+// Output pass with TMA (P = P1*P2 = 1024, split as in zdtf_output2_kernel): a persistent
+// grid, two CTAs per SM, walks the (rate pair, 8-residue) tiles; each tile's W (1024 k1
+// rows x 8 complex, 64 KB) is fetched by the tensor-memory accelerator as four 256-row
+// boxes completing on an mbarrier.  Waits on the mbarrier are bounded by kTmaWaitNs of
+// %globaltimer; a wait that runs out sets g_fused_fault and the CTA returns (reported by
+// fdr_synchronize).
 // ------------------------------------------------------------------------------------
 __device__ int g_fused_fault;
 constexpr unsigned long long kTmaWaitNs = 1000000000ull;  // 1 s
@@ -863,87 +862,74 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
       : "memory");
 }
 
+// The W tile lands (TMA) in a region that pass 1 then overwrites with its transposed
+// output, so a CTA needs ~76 KB and two fit per SM; the next tile's fetch is issued as soon
+// as pass 2 has read the region, overlapping pass 2's DFTs and FDR stores (and the other
+// CTA's work).
 template <int P1, int P2, int TS>
 struct OutTmaShape {
   static constexpr int P = P1 * P2;
   static constexpr int T = TS * (P1 > P2 ? P1 : P2);
   static constexpr int S1 = P2 + 1;
   static constexpr int SSEQ = ((P1 * S1 + 15) / 16) * 16 + 2;
-  static constexpr int BOXR = 256;                 // k1 rows per TMA box
+  static constexpr int BOXR = 256;
   static constexpr int NBOX = P / BOXR;
-  static constexpr unsigned STAGE = sizeof(float2) * P * TS;  // bytes of one W tile
-  static constexpr size_t SMEM = 1024 + 2 * (size_t)STAGE + sizeof(float2) * (TS * SSEQ + P) + 16;
-  static_assert(P % BOXR == 0 && TS * 2 * sizeof(float) % 16 == 0, "TMA box shape");
+  static constexpr unsigned TILEB = sizeof(float2) * P * TS;
+  static constexpr size_t REGION = sizeof(float2) * TS * SSEQ > TILEB ? sizeof(float2) * TS * SSEQ : TILEB;
+  static constexpr size_t SMEM = 128 + ((REGION + 127) / 128) * 128 + sizeof(float2) * P + 16;
+  static constexpr int MINB = 2;  // CTAs per SM
 };
 
 template <int P1, int P2, int TS>
-__global__ void __launch_bounds__(OutTmaShape<P1, P2, TS>::T, 1)
+__global__ void __launch_bounds__(OutTmaShape<P1, P2, TS>::T, OutTmaShape<P1, P2, TS>::MINB)
 zdtf_output_tma_kernel(const __grid_constant__ CUtensorMap wmap, long long N, int Q, int Nr,
-                       int npairs, float* __restrict__ dest, const float2* __restrict__ rootsP,
-                       double* __restrict__ acc) {
+                        int npairs, float* __restrict__ dest, const float2* __restrict__ rootsP,
+                        double* __restrict__ acc) {
   using SH = OutTmaShape<P1, P2, TS>;
   constexpr int P = SH::P, S1 = SH::S1, SSEQ = SH::SSEQ;
   extern __shared__ unsigned char smraw[];
-  const uintptr_t base = ((uintptr_t)smraw + 1023) & ~(uintptr_t)1023;
-  float2* stage0 = (float2*)base;
-  float2* stage1 = (float2*)(base + SH::STAGE);
-  float2* buf = (float2*)(base + 2 * (size_t)SH::STAGE);
-  float2* roots = buf + TS * SSEQ;  // exp(-2 pi i m / P)
+  const uintptr_t base = ((uintptr_t)smraw + 127) & ~(uintptr_t)127;
+  float2* region = (float2*)base;
+  float2* roots = (float2*)(base + ((SH::REGION + 127) / 128) * 128);
   unsigned long long* bar = (unsigned long long*)(roots + P);
   const int tid = threadIdx.x;
   const int ntna = Q / TS;
   const long long ntiles = (long long)ntna * npairs;
   if (tid == 0) {
     mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   for (int i = tid; i < P; i += SH::T) roots[i] = __ldg(rootsP + i);
   __syncthreads();
-  auto issue = [&](long long tile, int st) {  // thread 0 only
+  auto issue = [&](long long tile) {  // thread 0 only
     const int q = (int)(tile / ntna), nat = (int)(tile - (long long)q * ntna);
-    float2* dst = st ? stage1 : stage0;
-    mbar_expect_tx(&bar[st], SH::STAGE);
+    mbar_expect_tx(&bar[0], SH::TILEB);
 #pragma unroll
     for (int b = 0; b < SH::NBOX; ++b)
-      tma_load_2d(dst + b * SH::BOXR * TS, &wmap, 2 * TS * nat, q * P + b * SH::BOXR, &bar[st]);
+      tma_load_2d(region + b * SH::BOXR * TS, &wmap, 2 * TS * nat, q * P + b * SH::BOXR, &bar[0]);
   };
   const long long first = blockIdx.x, stride = gridDim.x;
-  if (tid == 0) {
-    if (first < ntiles) issue(first, 0);
-    if (first + stride < ntiles) issue(first + stride, 1);
-  }
+  if (tid == 0 && first < ntiles) issue(first);
   const int seq = tid % TS;
-  const int r = tid / TS;  // k1a in pass 1, nb_b in pass 2
+  const int r = tid / TS;
   int it = 0;
   for (long long tile = first; tile < ntiles; tile += stride, ++it) {
-    const int st = it & 1;
-    const unsigned parity = (unsigned)((it >> 1) & 1);
-    const bool ok = mbar_wait_bounded(&bar[st], parity);
+    const bool ok = mbar_wait_bounded(&bar[0], (unsigned)(it & 1));
     if (__syncthreads_or(!ok)) {
-      if (tid == 0) {
-        atomicOr(&g_fused_fault, 1);
-        // the other buffer's copy, if one was issued, before the shared memory goes away
-        if (tile + stride < ntiles) (void)mbar_wait_bounded(&bar[st ^ 1], (unsigned)(((it + 1) >> 1) & 1));
-      }
+      if (tid == 0) atomicOr(&g_fused_fault, 1);
       return;
     }
-    const float2* stg = st ? stage1 : stage0;
     const int q = (int)(tile / ntna), nat = (int)(tile - (long long)q * ntna);
     const int na0 = nat * TS;
     float2 v[P2];
     if (r < P1) {
 #pragma unroll
-      for (int m = 0; m < P2; ++m) v[m] = stg[(r + P1 * m) * TS + seq];
+      for (int m = 0; m < P2; ++m) v[m] = region[(r + P1 * m) * TS + seq];
     }
-    __syncthreads();  // this buffer is read: refill it with the next-but-one tile
-    if (tid == 0 && tile + 2 * stride < ntiles) {
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      issue(tile + 2 * stride, st);
-    }
+    __syncthreads();  // the tile is in registers: the region takes the transpose
     if (r < P1) {
       Dft<P2>::run(v, +1);
-      float2* b = buf + seq * SSEQ + r * S1;
+      float2* b = region + seq * SSEQ + r * S1;
 #pragma unroll
       for (int nbb = 0; nbb < P2; ++nbb) {
         const float2 t = roots[(r * nbb) & (P - 1)];
@@ -953,12 +939,19 @@ zdtf_output_tma_kernel(const __grid_constant__ CUtensorMap wmap, long long N, in
     __syncthreads();
     const int j = 2 * q;
     const bool has1 = (j + 1) < Nr;
-    double m[4] = {0.0, 0.0, 0.0, 0.0};
+    float2 w[P1];
     if (r < P2) {
-      float2 w[P1];
-      const float2* b = buf + seq * SSEQ + r;
+      const float2* b = region + seq * SSEQ + r;
 #pragma unroll
       for (int k1a = 0; k1a < P1; ++k1a) w[k1a] = b[k1a * S1];
+    }
+    __syncthreads();  // the region is read: fetch the next tile into it
+    if (tid == 0 && tile + stride < ntiles) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      issue(tile + stride);
+    }
+    double m[4] = {0.0, 0.0, 0.0, 0.0};
+    if (r < P2) {
       Dft<P1>::run(w, +1);
       float* d0 = dest + (long long)j * N + na0 + seq + (long long)Q * r;
       float* d1 = d0 + N;
@@ -976,7 +969,7 @@ zdtf_output_tma_kernel(const __grid_constant__ CUtensorMap wmap, long long N, in
         }
       }
     }
-    if (acc) {  // block reduction of the column moments, then one atomic add per value
+    if (acc) {
 #pragma unroll
       for (int i = 0; i < 4; ++i)
         for (int o = 16; o > 0; o >>= 1) m[i] += __shfl_down_sync(0xffffffffu, m[i], o);
@@ -990,8 +983,8 @@ zdtf_output_tma_kernel(const __grid_constant__ CUtensorMap wmap, long long N, in
         for (int i = 0; i < SH::T / 32; ++i) t += red[tid][i];
         if (tid < 2 || has1) atomicAdd(acc + 2 * j + tid, t);
       }
+      __syncthreads();  // red is free for the next tile
     }
-    __syncthreads();  // buf (and red) are free for the next tile
   }
 }
 
@@ -1385,9 +1378,9 @@ int fused_output(const FusedPlan* st, const float2* W, float* dest, double* acc,
   if (P == 1024 && Q >= 8 && tma_output_enabled()) {
     CUtensorMap map;
     if (w_tensor_map(&map, W, Q, st->npairs * (int64_t)P, 8)) {
-      using SH = OutTmaShape<32, 32, 8>;
       const long long ntiles = (long long)(Q / 8) * st->npairs;
-      const int grid = (int)std::min<long long>(ntiles, sm_count());
+      using SH = OutTmaShape<32, 32, 8>;
+      const int grid = (int)std::min<long long>(ntiles, (long long)SH::MINB * sm_count());
       zdtf_output_tma_kernel<32, 32, 8><<<grid, SH::T, SH::SMEM, s>>>(
           map, st->N, Q, (int)st->Nr, (int)st->npairs, dest, st->tab.rootsP, acc);
       FDR_LAUNCH_CHECK("zdtf_output_tma_kernel");
