@@ -123,6 +123,36 @@ def taylor_leg(fdr, torch, spec_dev, steps=20):
             "taylor_gbs_algorithmic": alg / (t_tree * 1e-3) / 1e9}
 
 
+def mixed_leg(fdr, torch, spec_dev, steps=20):
+    """The mixed-precision form (split-bfloat16 tensor-core DFTs in the output pass) on the
+    bench workload: device time per call and its relative L-infinity / L2 difference from the
+    float32 form on the same spectrogram."""
+    ws32 = fdr.ZDTWorkspace(spec_dev, R0, DR, NR)
+    wsm = fdr.ZDTWorkspace(spec_dev, R0, DR, NR, mixed_precision=True)
+    a, b = fdr.fortran_empty(NF, NR), fdr.fortran_empty(NF, NR)
+    fdr.zdtfdr_(a, ws32, spec_dev)
+    for _ in range(3):
+        fdr.zdtfdr_(b, wsm, spec_dev)
+    wsm.set_timing(True)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        fdr.zdtfdr_(b, wsm, spec_dev)
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    stages = {k: v / steps for k, v in wsm.stage_times()}
+    wsm.set_timing(False)
+    fdr.fdrsynchronize()
+    diff = (b - a)
+    linf = float(diff.abs().max() / a.abs().max())
+    l2 = float(diff.norm() / a.norm())
+    return {"form": "output DFT_P as split-bf16 mma.sync contractions, fp32 accumulation",
+            "ms_per_call": ms, "cells_per_s": NF * NR / (ms * 1e-3), "stages_ms": stages,
+            "rel_linf_vs_fp32": linf, "rel_l2_vs_fp32": l2}
+
+
 def ingest_leg(fdr, torch, host_specs):
     """File-to-hits pipeline: a SIGPROC filterbank of len(host_specs) coarse channels (the
     bench spectrograms side by side, Nf=2^20 fine channels each, Nt=16) in the page cache,
@@ -343,6 +373,8 @@ def main():
                     help="skip the batched multi-channel leg (64 uneven coarse channels)")
     ap.add_argument("--no-proposal", action="store_true",
                     help="skip the learned rate-window proposal leg")
+    ap.add_argument("--no-mixed", action="store_true",
+                    help="skip the mixed-precision (tensor-core output pass) leg")
     ap.add_argument("--no-ingest", action="store_true",
                     help="skip the filterbank-file search pipeline leg")
     ap.add_argument("--no-taylor", action="store_true",
@@ -479,6 +511,7 @@ def main():
     if not args.no_batched:
         batched = batched_leg(fdr, torch, max(3, min(args.steps, 10)))
     taylor = taylor_leg(fdr, torch, specs[0]) if rank == 0 and not args.no_taylor else None
+    mixed = mixed_leg(fdr, torch, specs[0]) if rank == 0 and not args.no_mixed else None
     ingest = ingest_leg(fdr, torch, host_specs) if rank == 0 and not args.no_ingest else None
     proposal = None
     if rank == 0 and not args.no_proposal:
@@ -525,6 +558,7 @@ def main():
             "batched": batched,
             "proposal": proposal,
             "taylor": taylor,
+            "mixed": mixed,
             "ingest": ingest,
         }
         print(json.dumps(line), flush=True)

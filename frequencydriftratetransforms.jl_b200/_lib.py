@@ -28,6 +28,7 @@ FDR_WINDOW_CUSTOM = 2
 FDR_ZDT_OUTPUT_ALIGNED = 0x1
 FDR_ZDT_EXACT_PHASE = 0x2
 FDR_ZDT_STAGED_ONLY = 0x4
+FDR_ZDT_MIXED_PRECISION = 0x8
 
 FDR_RATES_F64 = 0
 FDR_RATES_F32 = 1

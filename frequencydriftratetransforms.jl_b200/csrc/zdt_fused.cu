@@ -26,6 +26,7 @@
 // integer arithmetic modulo 2^bits; only the final conversion to a float in [-1, 1)
 // half-turns rounds.
 #include <cuda.h>  // CUtensorMap (the encode entry point is fetched from the runtime)
+#include <cuda_bf16.h>
 #include <cudaTypedefs.h>
 #include <math.h>
 #include <string.h>
@@ -989,6 +990,245 @@ zdtf_output_tma_kernel(const __grid_constant__ CUtensorMap wmap, long long N, in
 }
 
 // ------------------------------------------------------------------------------------
+// Mixed-precision output pass (workspace flag FDR_ZDT_MIXED_PRECISION; P = 1024 = 32 x 32).
+// Both radix-32 stages of the inverse DFT_P run as tensor-core contractions: per tile
+// (rate pair, 8 residues) C (64 x 256) = A (64 x 64) * B (64 x 256), where A is the real
+// embedding [[Re D, -Im D], [Im D, Re D]] of the 32-point inverse DFT matrix D and B holds
+// the real and imaginary parts of the 256 sequences (32 values each).  Operands are split
+// into bfloat16 pairs x = hi + lo (hi = bf16(x), lo = bf16(x - hi)) and C accumulates
+// hi*hi + hi*lo + lo*hi in float32 with mma.sync m16n8k16 (the lo*lo term, ~2^-16 relative,
+// is dropped).  The inter-stage twiddles, the statistics and the stores stay in float32 /
+// float64.  W tiles arrive by TMA into a double buffer as in zdtf_output_tma_kernel.
+// ------------------------------------------------------------------------------------
+struct OutMmaShape {
+  static constexpr int P = 1024, TS = 8, T = 256;
+  static constexpr unsigned STAGE = sizeof(float2) * P * TS;            // 64 KB
+  static constexpr int NFRAG = 16;                                      // 4 M-tiles x 4 K-tiles
+  static constexpr size_t AFRAG = (size_t)NFRAG * 32 * 2 * sizeof(uint4);  // hi + lo per lane
+  static constexpr size_t SMEM = 1024 + 2 * (size_t)STAGE + AFRAG + sizeof(float2) * (P + 32) + 16;
+};
+
+__device__ __forceinline__ unsigned bf16_pair(float a, float b) {  // a in the low half
+  __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
+  return *reinterpret_cast<unsigned*>(&v);
+}
+__device__ __forceinline__ float bf16_round(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
+
+__device__ __forceinline__ void mma_bf16_16816(float (&d)[4], const uint4& a, unsigned b0, unsigned b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a.x), "r"(a.y), "r"(a.z), "r"(a.w), "r"(b0), "r"(b1));
+}
+
+// Element (i, k) of the 64 x 64 real embedding of D[a][b] = exp(+2 pi i a b / 32).
+__device__ __forceinline__ float dft32_embed(int i, int k, const float2* cs) {
+  const float2 e = cs[((i & 31) * (k & 31)) & 31];  // (cos, sin)
+  if (i < 32) return k < 32 ? e.x : -e.y;
+  return k < 32 ? e.y : e.x;
+}
+
+// B fragments (hi, lo) of this warp's 4 column tiles for all 4 K-tiles, from a [32][256]
+// complex matrix in shared memory (real K rows 0..31 = real parts, 32..63 = imaginary).
+__device__ __forceinline__ void load_b_frags(const float2* src, int col0, int g, int t,
+                                             unsigned (&bh)[4][4][2], unsigned (&bl)[4][4][2]) {
+#pragma unroll
+  for (int kt = 0; kt < 2; ++kt) {
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt) {
+      const int c = col0 + nt * 8 + g;
+      const float2 v0 = src[(kt * 16 + 2 * t) * 256 + c];
+      const float2 v1 = src[(kt * 16 + 2 * t + 1) * 256 + c];
+      const float2 v8 = src[(kt * 16 + 2 * t + 8) * 256 + c];
+      const float2 v9 = src[(kt * 16 + 2 * t + 9) * 256 + c];
+      // real parts -> K-tile kt, imaginary parts -> K-tile kt + 2
+      float h0 = bf16_round(v0.x), h1 = bf16_round(v1.x), h8 = bf16_round(v8.x), h9 = bf16_round(v9.x);
+      bh[kt][nt][0] = bf16_pair(h0, h1);
+      bh[kt][nt][1] = bf16_pair(h8, h9);
+      bl[kt][nt][0] = bf16_pair(v0.x - h0, v1.x - h1);
+      bl[kt][nt][1] = bf16_pair(v8.x - h8, v9.x - h9);
+      h0 = bf16_round(v0.y); h1 = bf16_round(v1.y); h8 = bf16_round(v8.y); h9 = bf16_round(v9.y);
+      bh[kt + 2][nt][0] = bf16_pair(h0, h1);
+      bh[kt + 2][nt][1] = bf16_pair(h8, h9);
+      bl[kt + 2][nt][0] = bf16_pair(v0.y - h0, v1.y - h1);
+      bl[kt + 2][nt][1] = bf16_pair(v8.y - h8, v9.y - h9);
+    }
+  }
+}
+
+// C[mt][nt] = A * B over the 4 K-tiles, three split products each.
+__device__ __forceinline__ void mma_pass(const uint4* afrag, int lane, const unsigned (&bh)[4][4][2],
+                                         const unsigned (&bl)[4][4][2], float (&c)[4][4][4]) {
+#pragma unroll
+  for (int mt = 0; mt < 4; ++mt) {
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) c[mt][nt][e] = 0.f;
+#pragma unroll
+    for (int kt = 0; kt < 4; ++kt) {
+      const uint4 ah = afrag[((mt * 4 + kt) * 32 + lane) * 2];
+      const uint4 al = afrag[((mt * 4 + kt) * 32 + lane) * 2 + 1];
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) {
+        mma_bf16_16816(c[mt][nt], al, bh[kt][nt][0], bh[kt][nt][1]);
+        mma_bf16_16816(c[mt][nt], ah, bl[kt][nt][0], bl[kt][nt][1]);
+        mma_bf16_16816(c[mt][nt], ah, bh[kt][nt][0], bh[kt][nt][1]);
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(OutMmaShape::T, 1)
+zdtf_output_mma_kernel(const __grid_constant__ CUtensorMap wmap, long long N, int Q, int Nr, int npairs,
+                       float* __restrict__ dest, const float2* __restrict__ rootsP,
+                       double* __restrict__ acc) {
+  using SH = OutMmaShape;
+  constexpr int P = SH::P, TS = SH::TS;
+  extern __shared__ unsigned char smraw[];
+  const uintptr_t base = ((uintptr_t)smraw + 1023) & ~(uintptr_t)1023;
+  float2* stage0 = (float2*)base;
+  float2* stage1 = (float2*)(base + SH::STAGE);
+  uint4* afrag = (uint4*)(base + 2 * (size_t)SH::STAGE);
+  float2* roots = (float2*)(base + 2 * (size_t)SH::STAGE + SH::AFRAG);  // exp(-2 pi i m / P)
+  float2* cs = roots + P;                                                // cos, sin of 2 pi m / 32
+  unsigned long long* bar = (unsigned long long*)(cs + 32);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int ntna = Q / TS;
+  const long long ntiles = (long long)ntna * npairs;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  for (int i = tid; i < P; i += SH::T) roots[i] = __ldg(rootsP + i);
+  if (tid < 32) {
+    float sn, cn;
+    sincospif((float)tid / 16.f, &sn, &cn);
+    cs[tid] = make_float2(cn, sn);
+  }
+  __syncthreads();
+  // A fragments of the 16 (M-tile, K-tile) blocks, hi and lo, in the mma.sync m16n8k16 layout
+  for (int e = tid; e < SH::NFRAG * 32; e += SH::T) {
+    const int f = e >> 5, ln = e & 31, mt = f >> 2, kt = f & 3;
+    const int gg = ln >> 2, tt = ln & 3;
+    float v[8];
+    const int rows[8] = {gg, gg, gg + 8, gg + 8, gg, gg, gg + 8, gg + 8};
+    const int cols[8] = {2 * tt, 2 * tt + 1, 2 * tt, 2 * tt + 1, 2 * tt + 8, 2 * tt + 9, 2 * tt + 8, 2 * tt + 9};
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = dft32_embed(mt * 16 + rows[q], kt * 16 + cols[q], cs);
+    float h[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) h[q] = bf16_round(v[q]);
+    afrag[e * 2] = make_uint4(bf16_pair(h[0], h[1]), bf16_pair(h[2], h[3]), bf16_pair(h[4], h[5]),
+                              bf16_pair(h[6], h[7]));
+    afrag[e * 2 + 1] = make_uint4(bf16_pair(v[0] - h[0], v[1] - h[1]), bf16_pair(v[2] - h[2], v[3] - h[3]),
+                                  bf16_pair(v[4] - h[4], v[5] - h[5]), bf16_pair(v[6] - h[6], v[7] - h[7]));
+  }
+  __syncthreads();
+  auto issue = [&](long long tile, int st) {  // thread 0 only
+    const int q = (int)(tile / ntna), nat = (int)(tile - (long long)q * ntna);
+    float2* dst = st ? stage1 : stage0;
+    mbar_expect_tx(&bar[st], SH::STAGE);
+#pragma unroll
+    for (int b = 0; b < P / 256; ++b)
+      tma_load_2d(dst + b * 256 * TS, &wmap, 2 * TS * nat, q * P + b * 256, &bar[st]);
+  };
+  const long long first = blockIdx.x, stride = gridDim.x;
+  if (tid == 0) {
+    if (first < ntiles) issue(first, 0);
+    if (first + stride < ntiles) issue(first + stride, 1);
+  }
+  const int col0 = warp * 32;
+  int it = 0;
+  for (long long tile = first; tile < ntiles; tile += stride, ++it) {
+    const int st = it & 1;
+    const bool ok = mbar_wait_bounded(&bar[st], (unsigned)((it >> 1) & 1));
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) {
+        atomicOr(&g_fused_fault, 4);
+        if (tile + stride < ntiles) (void)mbar_wait_bounded(&bar[st ^ 1], (unsigned)(((it + 1) >> 1) & 1));
+      }
+      return;
+    }
+    float2* stg = st ? stage1 : stage0;
+    const int q = (int)(tile / ntna), nat = (int)(tile - (long long)q * ntna);
+    const int na0 = nat * TS;
+    unsigned bh[4][4][2], bl[4][4][2];
+    float c[4][4][4];
+    // pass 1: sequences (r = k1 mod 32, seq) over m = k1 / 32; column c = r*8 + seq, row m
+    load_b_frags(stg, col0, g, t, bh, bl);
+    __syncthreads();  // the tile is in registers: the stage takes the transposed result
+    mma_pass(afrag, lane, bh, bl, c);
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int nbb = mt * 16 + g + (e >= 2 ? 8 : 0);
+          const int col = col0 + nt * 8 + 2 * t + (e & 1);
+          const int r = col >> 3, seq = col & 7;
+          const float re = c[mt][nt][e], im = c[mt + 2][nt][e];
+          const float2 w = roots[(r * nbb) & (P - 1)];  // multiply by conj(w) = exp(+2 pi i r nbb / P)
+          stg[r * 256 + nbb * 8 + seq] = make_float2(re * w.x + im * w.y, im * w.x - re * w.y);
+        }
+    __syncthreads();
+    // pass 2: sequences (nbb, seq) over k1a = r; column c = nbb*8 + seq, row r
+    load_b_frags(stg, col0, g, t, bh, bl);
+    __syncthreads();  // the stage is read: refill it with the tile after next
+    if (tid == 0 && tile + 2 * stride < ntiles) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      issue(tile + 2 * stride, st);
+    }
+    mma_pass(afrag, lane, bh, bl, c);
+    const int j = 2 * q;
+    const bool has1 = (j + 1) < Nr;
+    double m[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int nba = mt * 16 + g + 8 * h;
+          const int col = col0 + nt * 8 + 2 * t;
+          const int nbb = col >> 3, seq = col & 7;
+          const long long n = (long long)(na0 + seq) + (long long)Q * (nbb + 32 * nba);
+          const float x0 = c[mt][nt][2 * h], x1 = c[mt][nt][2 * h + 1];
+          const float y0 = c[mt + 2][nt][2 * h], y1 = c[mt + 2][nt][2 * h + 1];
+          __stcs(reinterpret_cast<float2*>(dest + (long long)j * N + n), make_float2(x0, x1));
+          if (has1) __stcs(reinterpret_cast<float2*>(dest + (long long)(j + 1) * N + n), make_float2(y0, y1));
+          if (acc) {
+            m[0] += (double)x0 + (double)x1;
+            m[1] += (double)x0 * x0 + (double)x1 * x1;
+            if (has1) {
+              m[2] += (double)y0 + (double)y1;
+              m[3] += (double)y0 * y0 + (double)y1 * y1;
+            }
+          }
+        }
+    if (acc) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        for (int o = 16; o > 0; o >>= 1) m[i] += __shfl_down_sync(0xffffffffu, m[i], o);
+      __shared__ double red[4][SH::T / 32];
+      if (lane == 0)
+        for (int i = 0; i < 4; ++i) red[i][warp] = m[i];
+      __syncthreads();
+      if (tid < 4) {
+        double tt2 = 0.0;
+        for (int i = 0; i < SH::T / 32; ++i) tt2 += red[tid][i];
+        if (tid < 2 || has1) atomicAdd(acc + 2 * j + tid, tt2);
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------
 // Host side
 // ------------------------------------------------------------------------------------
 // Tile (sequences per CTA) and block size of kernels A and C for a given P: one radix-16
@@ -1120,6 +1360,8 @@ static int set_smem_attrs() {
                                 (int)Out2Shape<P1, P2, 8>::SMEM));
   SET_C2(8, 8) SET_C2(8, 16) SET_C2(16, 16) SET_C2(16, 32) SET_C2(32, 32)
 #undef SET_C2
+  FDR_CUDA(cudaFuncSetAttribute(zdtf_output_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)OutMmaShape::SMEM));
   FDR_CUDA(cudaFuncSetAttribute(zdtf_output_tma_kernel<32, 32, 8>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)OutTmaShape<32, 32, 8>::SMEM));
@@ -1373,6 +1615,23 @@ int fused_take_fault() {
   return FDR_OK;
 }
 
+// The output pass with the split-bfloat16 tensor-core DFTs (P = 1024 only; other shapes and a
+// failed tensor-map encode use the float32 kernels).
+int fused_output_mixed(const FusedPlan* st, const float2* W, float* dest, double* acc, cudaStream_t s) {
+  if (st->P == 1024 && st->Q >= 8) {
+    CUtensorMap map;
+    if (w_tensor_map(&map, W, st->Q, st->npairs * (int64_t)st->P, 8)) {
+      const long long ntiles = (long long)(st->Q / 8) * st->npairs;
+      const int grid = (int)std::min<long long>(ntiles, sm_count());
+      zdtf_output_mma_kernel<<<grid, OutMmaShape::T, OutMmaShape::SMEM, s>>>(
+          map, st->N, st->Q, (int)st->Nr, (int)st->npairs, dest, st->tab.rootsP, acc);
+      FDR_LAUNCH_CHECK("zdtf_output_mma_kernel");
+      return FDR_OK;
+    }
+  }
+  return fused_output(st, W, dest, acc, s);
+}
+
 int fused_output(const FusedPlan* st, const float2* W, float* dest, double* acc, cudaStream_t s) {
   const int P = st->P, Q = st->Q;
   if (P == 1024 && Q >= 8 && tma_output_enabled()) {
@@ -1457,7 +1716,8 @@ int zdt_fused_run(fdr_zdt* ws, float r0, float* dest, int window, const double* 
   }
   FDR_TRY(fused_czt(st, ws->A, ws->W, r0, ws->dr, window, wk, 0, s));
   zdt_mark(ws, "czt", s);
-  FDR_TRY(fused_output(st, ws->W, dest, acc, s));
+  if (ws->flags & FDR_ZDT_MIXED_PRECISION) FDR_TRY(fused_output_mixed(st, ws->W, dest, acc, s));
+  else FDR_TRY(fused_output(st, ws->W, dest, acc, s));
   zdt_mark(ws, "output", s);
   return FDR_OK;
 }
@@ -1478,7 +1738,8 @@ int zdt_fused_run_blocks(fdr_zdt* ws, const int* blk_base, int64_t nblocks, floa
   sub.npairs = 4 * nblocks;
   FDR_TRY(fused_czt_blocks(&sub, ws->A, ws->W, ws->r0, ws->dr, window, wk, blk_base, 0, s));
   zdt_mark(ws, "czt", s);
-  FDR_TRY(fused_output(&sub, ws->W, dest, acc, s));
+  if (ws->flags & FDR_ZDT_MIXED_PRECISION) FDR_TRY(fused_output_mixed(&sub, ws->W, dest, acc, s));
+  else FDR_TRY(fused_output(&sub, ws->W, dest, acc, s));
   zdt_mark(ws, "output", s);
   return FDR_OK;
 }

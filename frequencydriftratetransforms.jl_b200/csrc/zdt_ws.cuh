@@ -71,6 +71,7 @@ int fused_czt_blocks(const FusedPlan* st, const float2* A, float2* W, float r0, 
                      int window, const double* wk, const int* blk_base, int groups,
                      cudaStream_t s);
 int fused_output(const FusedPlan* st, const float2* W, float* dest, double* acc, cudaStream_t s);
+int fused_output_mixed(const FusedPlan* st, const float2* W, float* dest, double* acc, cudaStream_t s);
 // Reads and clears the fused kernels' fault flag (a bounded TMA wait that ran out).
 int fused_take_fault();
 int zdt_fused_run_blocks(fdr_zdt* ws, const int* blk_base, int64_t nblocks, float* dest,

@@ -42,13 +42,15 @@ class ZDTWorkspace:
 
     ``spectrogram`` may be None to create an empty workspace of size (Nf, Nt) given by
     ``shape``.  Extra keyword flags: ``exact_phase`` (reduce chirp phases exactly instead
-    of reproducing the reference's Float32 arguments in the staged stages) and
-    ``staged_only`` (zdtfdr_ always runs the staged kernels).
+    of reproducing the reference's Float32 arguments in the staged stages),
+    ``staged_only`` (zdtfdr_ always runs the staged kernels) and ``mixed_precision`` (the
+    fused output pass, for P = 1024 shapes such as Nf = 2^20 with Nt <= 16, runs its DFTs
+    as split-bfloat16 tensor-core contractions: ~1e-5 relative error instead of ~1e-6).
     """
 
     def __init__(self, spectrogram, r0_or_rates, dr=None, Nr=None, factors=(2, 3, 5), *,
-                 output_aligned=False, exact_phase=False, staged_only=False, shape=None,
-                 stream=None):
+                 output_aligned=False, exact_phase=False, staged_only=False, mixed_precision=False,
+                 shape=None, stream=None):
         if dr is None:
             r0, dr, Nr = _range_params(r0_or_rates)
         else:
@@ -66,6 +68,8 @@ class ZDTWorkspace:
             flags |= _lib.FDR_ZDT_EXACT_PHASE
         if staged_only:
             flags |= _lib.FDR_ZDT_STAGED_ONLY
+        if mixed_precision:
+            flags |= _lib.FDR_ZDT_MIXED_PRECISION
         farr, nf = _lib.i64_array([int(f) for f in factors])
         h = C.c_void_p()
         _lib.check(_lib.lib().fdr_zdt_create(
