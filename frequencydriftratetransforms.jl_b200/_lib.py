@@ -80,6 +80,7 @@ SIGNATURES = {
     "fdr_status_string": (C.c_char_p, [INT]),
     "fdr_kernel_launches": (I64, []),
     "fdr_synchronize": (INT, [P]),
+    "fdr_selftest_bounded_wait": (INT, [I64, P]),
     "fdr_calc_nl": (I64, [I64, I64, C.POINTER(I64), INT]),
     "fdr_grow_nr": (I64, [I64, I64, C.POINTER(I64), INT]),
     "fdr_estimate_memory": (I64, [I64, I64, I64, I64, I64, C.POINTER(I64), INT]),

@@ -142,6 +142,11 @@ const char* fdr_status_string(int status) {
   }
 }
 
+int fdr_selftest_bounded_wait(int64_t limit_ns, fdr_stream_t stream) {
+  FDR_CHECK_ARG(limit_ns > 0 && limit_ns <= 1000000000LL, "selftest: limit must be in (0, 1 s]");
+  return fdr::bounded_wait_selftest((unsigned long long)limit_ns, (cudaStream_t)stream);
+}
+
 int fdr_synchronize(fdr_stream_t stream) {
   if (stream) {
     FDR_CUDA(cudaStreamSynchronize((cudaStream_t)stream));

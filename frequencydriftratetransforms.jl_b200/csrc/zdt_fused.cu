@@ -848,11 +848,25 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned 
       : "memory");
   return ok != 0;
 }
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity,
+                                                  unsigned long long limit_ns = kTmaWaitNs) {
   const unsigned long long t0 = global_ns();
   while (!mbar_try_wait(bar, parity))
-    if (global_ns() - t0 > kTmaWaitNs) return false;
+    if (global_ns() - t0 > limit_ns) return false;
   return true;
+}
+
+// Self-test of the bounded wait: one CTA waits on an mbarrier that nothing completes, gives
+// up after limit_ns and raises the fault flag exactly as the TMA kernels do.
+__global__ void bounded_wait_selftest_kernel(unsigned long long limit_ns) {
+  __shared__ unsigned long long bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  const bool ok = mbar_wait_bounded(&bar, 0u, limit_ns);
+  if (__syncthreads_or(!ok) && threadIdx.x == 0) atomicOr(&g_fused_fault, 8);
 }
 // 2-D tiled TMA load (no multicast) of box {x .. x+15 floats, y .. y+255 rows} into dst.
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y,
@@ -1564,21 +1578,25 @@ int fused_czt_blocks(const FusedPlan* st, const float2* A, float2* W, float r0, 
   return FDR_ERR_UNSUPPORTED_SIZE;
 }
 
-// cuTensorMapEncodeTiled from the driver, through the runtime (no link against libcuda).
+// cuTensorMapEncodeTiled from the driver, through the runtime (no link against libcuda);
+// looked up once per process (thread-safe static initialisation).
 static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  static bool tried = false;
-  if (!tried) {
-    tried = true;
+  static const PFN_cuTensorMapEncodeTiled_v12000 fn = []() -> PFN_cuTensorMapEncodeTiled_v12000 {
     void* p = nullptr;
     cudaDriverEntryPointQueryResult q;
     if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
             cudaSuccess && q == cudaDriverEntryPointSuccess)
-      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
-    else
-      (void)cudaGetLastError();
-  }
+      return (PFN_cuTensorMapEncodeTiled_v12000)p;
+    (void)cudaGetLastError();
+    return nullptr;
+  }();
   return fn;
+}
+
+int bounded_wait_selftest(unsigned long long limit_ns, cudaStream_t s) {
+  bounded_wait_selftest_kernel<<<1, 32, 0, s>>>(limit_ns);
+  FDR_LAUNCH_CHECK("bounded_wait_selftest_kernel");
+  return FDR_OK;
 }
 
 // Tensor map of W as a 2-D float32 array: rows (rate pair, k1) of 2*Q floats, 16 x 256 boxes.
@@ -1609,7 +1627,8 @@ int fused_take_fault() {
   if (h) {
     const int z = 0;
     (void)cudaMemcpyToSymbol(g_fused_fault, &z, sizeof(int));
-    set_error(FDR_ERR_CUDA, "fused output: a TMA wait timed out (the FDR is incomplete)");
+    set_error(FDR_ERR_CUDA, "a bounded TMA/mbarrier wait timed out (flags 0x%x; the FDR of that "
+              "call is incomplete)", h);
     return FDR_ERR_CUDA;
   }
   return FDR_OK;

@@ -74,6 +74,7 @@ int fused_output(const FusedPlan* st, const float2* W, float* dest, double* acc,
 int fused_output_mixed(const FusedPlan* st, const float2* W, float* dest, double* acc, cudaStream_t s);
 // Reads and clears the fused kernels' fault flag (a bounded TMA wait that ran out).
 int fused_take_fault();
+int bounded_wait_selftest(unsigned long long limit_ns, cudaStream_t s);
 int zdt_fused_run_blocks(fdr_zdt* ws, const int* blk_base, int64_t nblocks, float* dest,
                          int window, const double* wk, double* acc, cudaStream_t s);
 // timing helpers

@@ -78,8 +78,13 @@ const char* fdr_status_string(int status);
    counterpart in the reference; used to count device launches in benchmarks). */
 int64_t fdr_kernel_launches(void);
 /* fdrsynchronize (fdrutils.jl:129-130; CuArray method ext:26-28): synchronise `stream`
-   (NULL: the whole device). */
+   (NULL: the whole device).  Also reports, once, a bounded wait of the TMA-fed kernels that
+   ran out since the last call (FDR_ERR_CUDA; that call's FDR is incomplete). */
 int fdr_synchronize(fdr_stream_t stream);
+/* Self-test of that failure path (no counterpart in the reference): launches one CTA that
+   waits on an mbarrier nothing completes, gives up after limit_ns (<= 1 s) and raises the
+   fault flag, so that the next fdr_synchronize returns FDR_ERR_CUDA.  No GPU fault. */
+int fdr_selftest_bounded_wait(int64_t limit_ns, fdr_stream_t stream);
 
 /* ---------------------------------------------------------------------------------- */
 /* zdtutils.jl                                                                         */

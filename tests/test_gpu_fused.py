@@ -173,3 +173,20 @@ def test_tma_output_matches_register_output(fdr, oracle, monkeypatch):
         monkeypatch.delenv("FDR_NO_TMA")
         assert np.array_equal(a, b)
         assert ta == tb and np.array_equal(ha, hb)
+
+
+def test_bounded_wait_fault_is_reported(fdr, oracle):
+    """A bounded mbarrier wait that runs out (the self-test kernel waits on a barrier that
+    nothing completes, 10 ms) raises the fault flag; fdr_synchronize reports it once as
+    FDR_ERR_CUDA, and the device stays usable: the next ZDT is correct."""
+    import ctypes as C
+    fdr._lib.check(fdr._lib.lib().fdr_selftest_bounded_wait(10_000_000, C.c_void_p(None)))
+    with pytest.raises(fdr.FDRError, match="timed out"):
+        fdr.fdrsynchronize()
+    fdr.fdrsynchronize()  # reported once, then cleared
+    spec = _spec(oracle, 1 << 20, 16, seed=99)
+    ws = fdr.ZDTWorkspace(spec, -4.0, 1 / 16, 9)
+    out = fdr.zdtfdr(ws).cpu().numpy()
+    truth = oracle.fdr_truth(spec, [-4.0, -3.5])
+    assert oracle.rel_linf(out[:, [0, 8]], truth) < 1e-5
+    fdr.fdrsynchronize()
