@@ -55,6 +55,27 @@ def synth(seed):
     return spec
 
 
+def rank_seeds(rank, nbuf):
+    """Seeds of a rank's synthetic spectrograms: every rank searches its own channels."""
+    return [1000 * rank + i + 1 for i in range(nbuf)]
+
+
+def max_over_ranks(x, world, device=None):
+    """The largest of a per-rank float over all ranks (the slowest replica times the job)."""
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(units_per_step, steps, world, t_max_s):
+    """Whole-job throughput of `world` independent replicas: all units over the max time."""
+    return units_per_step * steps * world / t_max_s
+
+
 def algorithmic_bytes():
     return 4 * NF * NT + 4 * NF * NR
 
@@ -407,7 +428,7 @@ def main():
 
     # Inputs: 4 distinct spectrograms per rank resident in HBM (256 MiB > 126 MB L2).
     nbuf = 4
-    host_specs = [synth(1000 * rank + i + 1) for i in range(nbuf)]
+    host_specs = [synth(sd) for sd in rank_seeds(rank, nbuf)]
     specs = [fdr.as_device_f32(h) for h in host_specs]
     ws = fdr.ZDTWorkspace(specs[0], R0, DR, NR, staged_only=args.staged)
     dest = fdr.fortran_empty(NF, NR)
@@ -439,13 +460,9 @@ def main():
     clk = clocks.stop()
     ms_total = e0.elapsed_time(e1)
     ws.set_timing(False)
-    t_max = ms_total
-    if world > 1:
-        t = torch.tensor([ms_total], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
+    t_max = max_over_ranks(ms_total, world, dev)
     ms_step = t_max / args.steps
-    value = NF * NR * args.steps * world / (t_max * 1e-3)
+    value = replica_value(NF * NR, args.steps, world, t_max * 1e-3)
 
     # ---------------- end-to-end through the public API (host buffers) ----------------
     # Each step: pinned host spectrogram -> device (copy stream, double-buffered so the
@@ -490,12 +507,8 @@ def main():
     if e2e_steps:
         run_e2e(e2e_steps)
     torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = NF * NR * e2e_steps * world / e2e_s if e2e_steps else None
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world, dev)
+    e2e_value = replica_value(NF * NR, e2e_steps, world, e2e_s) if e2e_steps else None
 
     # ---------------- roofline of the ZDT call ----------------
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
