@@ -265,7 +265,7 @@ __device__ __forceinline__ float window_value(const CztArgs& a, long long k) {
 // Kernel B: grid (P/2, rate groups), Q/2 threads.
 // ------------------------------------------------------------------------------------
 template <int Q, int NTR>
-__global__ void __launch_bounds__(Q / 2, 1) zdtf_czt_kernel(CztArgs a) {
+__global__ void __launch_bounds__(Q / 2, (Q <= 512 ? 2 : 1)) zdtf_czt_kernel(CztArgs a) {
   constexpr int T = Q / 2;
   constexpr int SS = b_stride<Q>();
   extern __shared__ float2 sm[];
@@ -1004,6 +1004,162 @@ zdtf_output_tma_kernel(const __grid_constant__ CUtensorMap wmap, long long N, in
 }
 
 // ------------------------------------------------------------------------------------
+// Output pass with TMA for P = 2048 = 64 x 32 (the four-step split of Nf = 2^20 with 512
+// bins per czt CTA).  As zdtf_output_tma_kernel, with 8 residues per tile (2048 rows x
+// 64 B = 128 KB, one CTA of 512 threads per SM; tiles of 4 residues, 32-byte rows, two
+// CTAs per SM, measured 4x slower).  Pass 1: thread (seq, k1a < 64) transforms its 32
+// values over k1b.  Pass 2 (the 64-point DFT over k1a) is split between lanes h = 0, 1 of a
+// warp (decimation in time): lane h transforms the 32 values k1a = 2k + h, lane 1 applies
+// w_64^n, and the two exchange half of their results by shuffles, so every lane ends with
+// 32 of the 64 outputs.
+// Shared-memory strides: S1 = 33 (odd) and SSEQ = 16/TS (mod 16) keep the transposed
+// writes of pass 1 (TS seq x 16/TS k1a per half-warp) and the reads of pass 2 (TS seq x
+// 16/TS nb_b per half-warp, h fixed) on distinct bank pairs.
+// ------------------------------------------------------------------------------------
+template <int TS_>
+struct OutTma64Shape {
+  static constexpr int P1 = 64, P2 = 32, P = P1 * P2, TS = TS_, T = 64 * TS;
+  static constexpr int S1 = P2 + 1;
+  static constexpr int SSEQ = ((P1 * S1 + 15) / 16) * 16 + 16 / TS;
+  static constexpr int BOXR = 256;
+  static constexpr int NBOX = P / BOXR;
+  static constexpr unsigned TILEB = sizeof(float2) * P * TS;
+  static constexpr size_t REGION = sizeof(float2) * TS * SSEQ > TILEB ? sizeof(float2) * TS * SSEQ : TILEB;
+  static constexpr size_t SMEM = 128 + ((REGION + 127) / 128) * 128 + sizeof(float2) * P + 16;
+  static constexpr int MINB = TS <= 4 ? 2 : 1;
+};
+
+template <int TS_>
+__global__ void __launch_bounds__(OutTma64Shape<TS_>::T, OutTma64Shape<TS_>::MINB)
+zdtf_output_tma64_kernel(const __grid_constant__ CUtensorMap wmap, long long N, int Q, int Nr,
+                         int npairs, float* __restrict__ dest, const float2* __restrict__ rootsP,
+                         double* __restrict__ acc) {
+  using SH = OutTma64Shape<TS_>;
+  constexpr int P = SH::P, P1 = SH::P1, P2 = SH::P2, TS = SH::TS, S1 = SH::S1, SSEQ = SH::SSEQ;
+  extern __shared__ unsigned char smraw[];
+  const uintptr_t base = ((uintptr_t)smraw + 127) & ~(uintptr_t)127;
+  float2* region = (float2*)base;
+  float2* roots = (float2*)(base + ((SH::REGION + 127) / 128) * 128);
+  unsigned long long* bar = (unsigned long long*)(roots + P);
+  const int tid = threadIdx.x;
+  const int ntna = Q / TS;
+  const long long ntiles = (long long)ntna * npairs;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  for (int i = tid; i < P; i += SH::T) roots[i] = __ldg(rootsP + i);
+  __syncthreads();
+  auto issue = [&](long long tile) {  // thread 0 only
+    const int q = (int)(tile / ntna), nat = (int)(tile - (long long)q * ntna);
+    mbar_expect_tx(&bar[0], SH::TILEB);
+#pragma unroll
+    for (int b = 0; b < SH::NBOX; ++b)
+      tma_load_2d(region + b * SH::BOXR * TS, &wmap, 2 * TS * nat, q * P + b * SH::BOXR, &bar[0]);
+  };
+  const long long first = blockIdx.x, stride = gridDim.x;
+  if (tid == 0 && first < ntiles) issue(first);
+  // pass 1 roles
+  const int seq1 = tid % TS, r = tid / TS;  // r = k1a < 64
+  // pass 2 roles: lane = seq + TS * (nb_b mod (16 / TS)) + 16 * h
+  const int lane = tid & 31;
+  const int seq2 = lane % TS, h = lane >> 4;
+  const int nbb = ((lane / TS) % (16 / TS)) + (16 / TS) * (tid >> 5);
+  int it = 0;
+  for (long long tile = first; tile < ntiles; tile += stride, ++it) {
+    const bool ok = mbar_wait_bounded(&bar[0], (unsigned)(it & 1));
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) atomicOr(&g_fused_fault, 1);
+      return;
+    }
+    const int q = (int)(tile / ntna), nat = (int)(tile - (long long)q * ntna);
+    const int na0 = nat * TS;
+    float2 v[P2];
+#pragma unroll
+    for (int m = 0; m < P2; ++m) v[m] = region[(r + P1 * m) * TS + seq1];
+    __syncthreads();  // the tile is in registers: the region takes the transpose
+    Dft<P2>::run(v, +1);
+    {
+      float2* b = region + seq1 * SSEQ + r * S1;
+#pragma unroll
+      for (int n = 0; n < P2; ++n) {
+        const float2 t = roots[(r * n) & (P - 1)];
+        b[n] = cmul(v[n], make_float2(t.x, -t.y));
+      }
+    }
+    __syncthreads();
+    {
+      const float2* b = region + seq2 * SSEQ + h * S1 + nbb;
+#pragma unroll
+      for (int k = 0; k < P1 / 2; ++k) v[k] = b[2 * k * S1];
+    }
+    __syncthreads();  // the region is read: fetch the next tile into it
+    if (tid == 0 && tile + stride < ntiles) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      issue(tile + stride);
+    }
+    Dft<P1 / 2>::run(v, +1);  // E (h = 0) or O (h = 1) at n mod 32
+    if (h) {
+#pragma unroll
+      for (int n = 1; n < P1 / 2; ++n) {
+        const float2 t = roots[n * (P / P1)];  // exp(-2 pi i n / 64)
+        v[n] = cmul(v[n], make_float2(t.x, -t.y));
+      }
+    }
+    // lane 0-half keeps E[0..15] and receives w O[0..15]; lane 1-half keeps w O[16..31] and
+    // receives E[16..31]: z[n] = E[n] + w^n O[n], z[n + 32] = E[n] - w^n O[n]
+#pragma unroll
+    for (int i = 0; i < P1 / 4; ++i) {
+      const float2 s = h ? v[i] : v[i + P1 / 4];
+      float2 o;
+      o.x = __shfl_xor_sync(0xffffffffu, s.x, 16);
+      o.y = __shfl_xor_sync(0xffffffffu, s.y, 16);
+      const float2 e = h ? o : v[i];
+      const float2 w = h ? v[i + P1 / 4] : o;
+      v[i] = cadd(e, w);             // z[i + 16h]
+      v[i + P1 / 4] = csub(e, w);    // z[i + 16h + 32]
+    }
+    const int j = 2 * q;
+    const bool has1 = (j + 1) < Nr;
+    double m[4] = {0.0, 0.0, 0.0, 0.0};
+    {
+      float* d0 = dest + (long long)j * N + na0 + seq2 + (long long)Q * nbb;
+      float* d1 = d0 + N;
+#pragma unroll
+      for (int i = 0; i < P1 / 2; ++i) {
+        const int nba = (i & (P1 / 4 - 1)) + 16 * h + (i >= P1 / 4 ? P1 / 2 : 0);
+        const long long off = (long long)Q * P2 * nba;
+        __stcs(d0 + off, v[i].x);
+        if (has1) __stcs(d1 + off, v[i].y);
+      }
+      if (acc) {
+#pragma unroll
+        for (int i = 0; i < P1 / 2; ++i) {
+          const double x = v[i].x, y = has1 ? v[i].y : 0.f;
+          m[0] += x; m[1] += x * x; m[2] += y; m[3] += y * y;
+        }
+      }
+    }
+    if (acc) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        for (int o = 16; o > 0; o >>= 1) m[i] += __shfl_down_sync(0xffffffffu, m[i], o);
+      __shared__ double red[4][SH::T / 32];
+      const int wid = tid >> 5;
+      if ((tid & 31) == 0)
+        for (int i = 0; i < 4; ++i) red[i][wid] = m[i];
+      __syncthreads();
+      if (tid < 4) {
+        double t = 0.0;
+        for (int i = 0; i < SH::T / 32; ++i) t += red[tid][i];
+        if (tid < 2 || has1) atomicAdd(acc + 2 * j + tid, t);
+      }
+      __syncthreads();  // red is free for the next tile
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------
 // Mixed-precision output pass (workspace flag FDR_ZDT_MIXED_PRECISION; P = 1024 = 32 x 32).
 // Both radix-32 stages of the inverse DFT_P run as tensor-core contractions: per tile
 // (rate pair, 8 residues) C (64 x 256) = A (64 x 64) * B (64 x 256), where A is the real
@@ -1260,11 +1416,14 @@ struct CztShape {
       sizeof(float2) * (kRatesPerBlock * b_stride<Q>() + tw_size(Q) + 2 * Q + kFusedMaxNt);
 };
 
-// log2 of the four-step factor Q for Nf = 2^L and Nt time steps: up to 1024 bins per CTA
-// while F fits in registers (Nt <= 16), then 512 (Nt <= 32) and 256 (Nt <= 64) so that
-// F of the CTA's bins fits in shared memory.
-static int fused_qlog(int L, int64_t Nt) {
-  const int cap = Nt <= 16 ? 10 : (Nt <= 32 ? 9 : 8);
+// log2 of the four-step factor Q for Nf = 2^L and Nt time steps.  With F in registers
+// (Nt <= 16): 512 bins per CTA up to Nf = 2^20 (256 threads, two CTAs per SM, so one CTA's
+// barriers overlap the other's Horner sums; P <= 2048 keeps the TMA output passes), 1024
+// above; with F in shared memory 512 (Nt <= 32) and 256 (Nt <= 64).  p1024 (the
+// mixed-precision output pass, whose tensor-core DFTs are written for P = 1024) keeps 1024
+// bins per CTA for Nt <= 16, so that Nf = 2^20 splits as 1024 x 1024.
+static int fused_qlog(int L, int64_t Nt, bool p1024 = false) {
+  const int cap = Nt <= 16 ? ((L <= 20 && !p1024) ? 9 : 10) : (Nt <= 32 ? 9 : 8);
   return std::min(cap, (L + 1) / 2);
 }
 
@@ -1379,6 +1538,8 @@ static int set_smem_attrs() {
   FDR_CUDA(cudaFuncSetAttribute(zdtf_output_tma_kernel<32, 32, 8>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)OutTmaShape<32, 32, 8>::SMEM));
+  FDR_CUDA(cudaFuncSetAttribute(zdtf_output_tma64_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)OutTma64Shape<8>::SMEM));
 #define SET_B(Q)                                                                               \
   FDR_CUDA(cudaFuncSetAttribute(zdtf_czt_kernel<Q, kFusedMaxNt>,                               \
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CztShape<Q>::SMEM)); \
@@ -1400,7 +1561,7 @@ static int set_smem_attrs() {
   return FDR_OK;
 }
 
-int fused_plan_create(FusedPlan** out, int64_t N, int64_t Nt, int64_t Nr) {
+int fused_plan_create(FusedPlan** out, int64_t N, int64_t Nt, int64_t Nr, bool p1024) {
   *out = nullptr;
   if (!zdt_fused_eligible(N, Nt, Nr)) {
     set_error(FDR_ERR_UNSUPPORTED_SIZE, "fused plan: Nf=%lld Nt=%lld not supported",
@@ -1411,7 +1572,7 @@ int fused_plan_create(FusedPlan** out, int64_t N, int64_t Nt, int64_t Nr) {
   FusedPlan* st = new FusedPlan();
   st->N = N; st->Nt = Nt; st->Nr = Nr;
   st->L = ilog2(N);
-  const int Qlog = fused_qlog(st->L, Nt);
+  const int Qlog = fused_qlog(st->L, Nt, p1024);
   st->Q = 1 << Qlog;
   st->P = (int)(N >> Qlog);
   st->B = (st->L + 1) / 2;
@@ -1665,6 +1826,18 @@ int fused_output(const FusedPlan* st, const float2* W, float* dest, double* acc,
       return FDR_OK;
     }
   }
+  if (P == 2048 && Q >= 8 && tma_output_enabled()) {
+    CUtensorMap map;
+    using SH = OutTma64Shape<8>;
+    if (w_tensor_map(&map, W, Q, st->npairs * (int64_t)P, SH::TS)) {
+      const long long ntiles = (long long)(Q / SH::TS) * st->npairs;
+      const int grid = (int)std::min<long long>(ntiles, (long long)SH::MINB * sm_count());
+      zdtf_output_tma64_kernel<8><<<grid, SH::T, SH::SMEM, s>>>(
+          map, st->N, Q, (int)st->Nr, (int)st->npairs, dest, st->tab.rootsP, acc);
+      FDR_LAUNCH_CHECK("zdtf_output_tma64_kernel");
+      return FDR_OK;
+    }
+  }
 #define LAUNCH_C2(PP, P1, P2)                                                                  \
   if (P == PP) {                                                                               \
     using SH = Out2Shape<P1, P2, 8>;                                                           \
@@ -1698,7 +1871,7 @@ static FusedPlan* st_of(fdr_zdt* ws) { return reinterpret_cast<FusedPlan*>(ws->f
 
 int zdt_fused_setup(fdr_zdt* ws) {
   FusedPlan* st = nullptr;
-  FDR_TRY(fused_plan_create(&st, ws->Nf, ws->Nt, ws->Nr));
+  FDR_TRY(fused_plan_create(&st, ws->Nf, ws->Nt, ws->Nr, (ws->flags & FDR_ZDT_MIXED_PRECISION) != 0));
   ws->fstate = st;
   ws->fP = st->P;
   ws->fQ = st->Q;

@@ -56,7 +56,7 @@ void zdt_fused_release(fdr_zdt* ws);
 
 // Fused kernels for one (Nf, Nt, Nr) shape with caller-owned intermediates (zdt_fused.cu).
 struct FusedPlan;
-int fused_plan_create(FusedPlan** out, int64_t N, int64_t Nt, int64_t Nr);
+int fused_plan_create(FusedPlan** out, int64_t N, int64_t Nt, int64_t Nr, bool p1024 = false);
 void fused_plan_destroy(FusedPlan* st);
 int64_t fused_plan_table_bytes(const FusedPlan* st);
 int64_t fused_A_elems(const FusedPlan* st);

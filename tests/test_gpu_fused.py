@@ -156,10 +156,10 @@ def test_rate_blocks_argument_errors(fdr, oracle):
 
 
 def test_tma_output_matches_register_output(fdr, oracle, monkeypatch):
-    """The output pass with TMA-fed double buffering (P = 1024) writes the same FDR, bit for
-    bit, as the register-load output kernel (FDR_NO_TMA=1), with and without the fused
-    proto-hit statistics (odd Nt too), and reports no fault."""
-    for Nf, Nt, Nr in ((1 << 20, 16, 129), (1 << 18, 40, 33), (1 << 20, 15, 9)):
+    """The TMA-fed output pass for P = 1024 writes the same FDR, bit for bit, as the
+    register-load output kernel (FDR_NO_TMA=1) with the same 32 x 32 split, with and without
+    the fused proto-hit statistics (odd Nt too), and reports no fault."""
+    for Nf, Nt, Nr in ((1 << 19, 16, 129), (1 << 18, 40, 33), (1 << 19, 15, 9)):
         spec = _spec(oracle, Nf, Nt, seed=Nf + Nt + 5)
         ws = fdr.ZDTWorkspace(spec, -4.0, 1 / 16, Nr)
         a = fdr.zdtfdr(ws).cpu().numpy()
@@ -173,6 +173,32 @@ def test_tma_output_matches_register_output(fdr, oracle, monkeypatch):
         monkeypatch.delenv("FDR_NO_TMA")
         assert np.array_equal(a, b)
         assert ta == tb and np.array_equal(ha, hb)
+
+
+@pytest.mark.parametrize("Nf,Nt,Nr", [(1 << 20, 16, 129), (1 << 21, 16, 17), (1 << 20, 15, 9),
+                                      (1 << 20, 24, 33)])
+def test_tma_output_p2048(fdr, oracle, monkeypatch, Nf, Nt, Nr):
+    """The TMA-fed output pass for P = 2048 (64 x 32 split, the 64-point DFT shared by lane
+    pairs): FDR within float32 rounding of the shared-memory FFT output kernel
+    (FDR_NO_TMA=1) and of the FP64 direct sums on sampled columns, the proto-hits of that FDR
+    at the kernel's threshold and no fault."""
+    spec = _spec(oracle, Nf, Nt, seed=Nf + Nt + 7)
+    ws = fdr.ZDTWorkspace(spec, -4.0, 1 / 16, Nr)
+    a = fdr.zdtfdr(ws).cpu().numpy()
+    ha, ta = fdr.zdtfdr_protohits_(fdr.fortran_empty(Nf, Nr), ws, spec, threshold=8.0,
+                                   return_threshold=True)
+    fdr.fdrsynchronize()
+    monkeypatch.setenv("FDR_NO_TMA", "1")
+    b = fdr.zdtfdr(ws).cpu().numpy()
+    monkeypatch.delenv("FDR_NO_TMA")
+    scale = np.abs(b).max()
+    assert np.abs(a - b).max() <= 2e-6 * scale
+    cols = sorted({0, Nr // 2, Nr - 1})
+    truth = oracle.fdr_truth(spec, [-4.0 + j / 16 for j in cols])
+    assert oracle.rel_linf(a[:, cols], truth) < 1e-5
+    m, sd = oracle.fdrstats(a)
+    assert abs(ta - (8.0 * sd + m)) <= 1e-5 * abs(ta)
+    assert np.array_equal(ha, oracle.findprotohits(a, ta))
 
 
 def test_bounded_wait_fault_is_reported(fdr, oracle):
