@@ -235,9 +235,45 @@ __device__ __forceinline__ void stockham_pass(float2* buf, const float2* twt) {
   __syncthreads();
 }
 
+// One radix-R Stockham pass from src to dst (same layout, distinct buffers): each thread
+// transforms its butterflies one at a time; ends with a barrier.
+template <int LEN, int NSEQ, int SSTRIDE, int T, int SIGN, int NS, int R>
+__device__ __forceinline__ void stockham_pass_oop(const float2* src, float2* dst, const float2* twt) {
+  constexpr int NBF = LEN / R;
+  constexpr int NB = NBF * NSEQ;
+  constexpr int PER = (NB + T - 1) / T;
+  const float2* tw = twt + tw_offset(LEN, NS);
+#pragma unroll
+  for (int i = 0; i < PER; ++i) {
+    const int j = threadIdx.x + i * T;
+    if (NB % T == 0 || j < NB) {
+      const int seq = j / NBF, jj = j - seq * NBF;
+      const int k = jj % NS;
+      float2 v[R];
+      const float2* a = src + seq * SSTRIDE;
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[r] = a[pidx(jj + r * NBF)];
+      if (NS > 1) {
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          float2 w = tw[(r - 1) * NS + k];
+          if (SIGN > 0) w.y = -w.y;
+          v[r] = cmul(v[r], w);
+        }
+      }
+      Dft<R>::run(v, SIGN);
+      float2* b = dst + seq * SSTRIDE;
+      const int base = (jj / NS) * NS * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) b[pidx(base + r * NS)] = v[r];
+    }
+  }
+  __syncthreads();
+}
+
 // The last pass of an in-place Stockham FFT whose outputs go to emit(seq, i, value)
-// instead of shared memory (natural order i).  Ends with a barrier.
-template <int LEN, int NSEQ, int SSTRIDE, int T, int SIGN, int NS, int R, class Emit>
+// instead of shared memory (natural order i).  Ends with a barrier if SYNC.
+template <int LEN, int NSEQ, int SSTRIDE, int T, int SIGN, int NS, int R, class Emit, bool SYNC = true>
 __device__ __forceinline__ void stockham_last_pass_emit(float2* buf, const float2* twt, Emit emit) {
   constexpr int NBF = LEN / R;
   constexpr int NB = NBF * NSEQ;
@@ -267,7 +303,7 @@ __device__ __forceinline__ void stockham_last_pass_emit(float2* buf, const float
       for (int r = 0; r < R; ++r) emit(seq, base + r * NS, v[r]);
     }
   }
-  __syncthreads();
+  if (SYNC) __syncthreads();
 }
 
 template <int LEN, int NSEQ, int SSTRIDE, int T, int SIGN, int NS, class Emit>
@@ -279,6 +315,31 @@ __device__ __forceinline__ void stockham_passes_emit(float2* buf, const float2* 
   } else {
     stockham_last_pass_emit<LEN, NSEQ, SSTRIDE, T, SIGN, NS, R>(buf, twt, emit);
   }
+}
+
+// Ping-pong form of stockham_passes_emit: the passes alternate between buffers a and b
+// (a holds the input), the last pass reads whichever holds the data and hands its outputs
+// to emit; no barrier after it.  The buffer that the last pass does NOT read was last read
+// before the final barrier, so the caller may refill it at once.
+template <int LEN, int NSEQ, int SSTRIDE, int T, int SIGN, int NS, class Emit>
+__device__ __forceinline__ void stockham_passes_emit_pp(float2* a, float2* b, const float2* twt, Emit emit) {
+  constexpr int R = plan_radix(LEN / NS);
+  if constexpr (NS * R < LEN) {
+    stockham_pass_oop<LEN, NSEQ, SSTRIDE, T, SIGN, NS, R>(a, b, twt);
+    stockham_passes_emit_pp<LEN, NSEQ, SSTRIDE, T, SIGN, NS * R>(b, a, twt, emit);
+  } else {
+    stockham_last_pass_emit<LEN, NSEQ, SSTRIDE, T, SIGN, NS, R, Emit, false>(a, twt, emit);
+  }
+}
+
+// Number of shared-memory passes before the emitting pass of a length-LEN FFT.
+__host__ __device__ constexpr int passes_before_emit(int len) {
+  int n = 0, ns = 1;
+  while (ns * plan_radix(len / ns) < len) {
+    ns *= plan_radix(len / ns);
+    ++n;
+  }
+  return n;
 }
 
 // smem_fft whose final pass hands each output to emit(seq, i, value) (no shared store).

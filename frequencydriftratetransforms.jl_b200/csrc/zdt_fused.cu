@@ -273,6 +273,7 @@ __global__ void __launch_bounds__(Q / 2, (Q <= 512 ? 2 : 1)) zdtf_czt_kernel(Czt
   float2* twt = buf + kRatesPerBlock * SS;    // tw_size(Q)
   float2* twr = twt + tw_size(Q);             // 2 * Q
   float2* gnyq = twr + 2 * Q;                 // NTR
+  float2* buf2 = gnyq + NTR;                  // kRatesPerBlock * SS
   const int tid = threadIdx.x;
   const int c = blockIdx.x;
   const int P = a.P;
@@ -322,12 +323,17 @@ __global__ void __launch_bounds__(Q / 2, (Q <= 512 ? 2 : 1)) zdtf_czt_kernel(Czt
   for (int b = 0; b < 2; ++b) mirror_of(c, b, tid, Q, &ms[b], &mk2[b]);
   const bool dc = (c == 0 && tid == 0);
 
+  // Rate blocks alternate between buf2 and buf (the forward pass used buf): the inverse
+  // DFT_Q ping-pongs between the two, and the buffer a block's Horner sums go to was last
+  // read before the previous block's final barrier, so no barrier precedes the writes.
+  constexpr bool kFlip = (passes_before_emit(Q) % 2) == 0;
+  float2* hb = buf2;
+  float2* ob = buf;
   const int q_begin = blockIdx.y * a.pairs_per_group;
   const int q_end = min(a.npairs, q_begin + a.pairs_per_group);
   for (int q0 = q_begin; q0 < q_end; q0 += kRatesPerBlock / 2) {
     const int j0 = 2 * q0;
     const long long jg = a.blk_base ? (long long)__ldg(a.blk_base + (q0 >> 2)) : (long long)j0;
-    __syncthreads();  // buf is free
     // exact phase of the block's first rate; the second half starts at w0 * w(k, 4*dr)
     float2 Wbx, Wby;
     {
@@ -365,10 +371,10 @@ __global__ void __launch_bounds__(Q / 2, (Q <= 512 ? 2 : 1)) zdtf_czt_kernel(Czt
           const int u = h * (kHorner / 2) + u2;  // rate pair within the block
           const float2 sa = S[b][2 * u2], sb = S[b][2 * u2 + 1];
           if (dc && b == 0) {
-            buf[(2 * u) * SS + pidx(0)] = make_float2(sa.x, sb.x);  // real-only DC bin
+            hb[(2 * u) * SS + pidx(0)] = make_float2(sa.x, sb.x);  // real-only DC bin
           } else {
-            buf[(2 * u + b) * SS + pidx(tid)] = make_float2(sa.x - sb.y, sa.y + sb.x);          // sa + i sb
-            buf[(2 * u + ms[b]) * SS + pidx(mk2[b])] = make_float2(sa.x + sb.y, sb.x - sa.y);  // conj(sa) + i conj(sb)
+            hb[(2 * u + b) * SS + pidx(tid)] = make_float2(sa.x - sb.y, sa.y + sb.x);          // sa + i sb
+            hb[(2 * u + ms[b]) * SS + pidx(mk2[b])] = make_float2(sa.x + sb.y, sb.x - sa.y);  // conj(sa) + i conj(sb)
           }
         }
       }
@@ -387,18 +393,23 @@ __global__ void __launch_bounds__(Q / 2, (Q <= 512 ? 2 : 1)) zdtf_czt_kernel(Czt
           const float2 sv = horner<NTR>(Gn, w);
           v[hh] = (j < a.Nr) ? sv.x * wn : 0.f;  // real-only Nyquist bin
         }
-        buf[(2 * u) * SS + pidx(Q / 2)] = make_float2(v[0], v[1]);
+        hb[(2 * u) * SS + pidx(Q / 2)] = make_float2(v[0], v[1]);
       }
     }
     __syncthreads();
     // inverse DFT_Q; its last pass writes W (with the inter-pass twiddle and 1/Nf) directly
     float2* const W = a.W;
     const int k1a = k1s[0], k1b = k1s[1];
-    smem_fft_emit<Q, kRatesPerBlock, SS, T, +1>(buf, twt, [&](int seq, int na, float2 v) {
+    stockham_passes_emit_pp<Q, kRatesPerBlock, SS, T, +1, 1>(hb, ob, twt, [&](int seq, int na, float2 v) {
       const int q = q0 + (seq >> 1), side = seq & 1;
       if (q < q_end)
         W[((long long)q * P + (side ? k1b : k1a)) * Q + na] = cmul(v, twr[side * Q + na]);
     });
+    if (kFlip) {
+      float2* t = hb;
+      hb = ob;
+      ob = t;
+    }
   }
 }
 
@@ -1411,9 +1422,9 @@ struct AcShape {
 };
 
 template <int Q>
-struct CztShape {
+struct CztShape {  // buf | twt | twr | gnyq | buf2 (the second rate-block buffer)
   static constexpr size_t SMEM =
-      sizeof(float2) * (kRatesPerBlock * b_stride<Q>() + tw_size(Q) + 2 * Q + kFusedMaxNt);
+      sizeof(float2) * (2 * kRatesPerBlock * b_stride<Q>() + tw_size(Q) + 2 * Q + kFusedMaxNt);
 };
 
 // log2 of the four-step factor Q for Nf = 2^L and Nt time steps.  With F in registers
