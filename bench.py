@@ -471,7 +471,7 @@ def main():
     pinned = [torch.from_numpy(h.T.copy()).pin_memory() for h in host_specs]  # (Nt, Nf) rows
     dev_in = [fdr.fortran_empty(NF, NT) for _ in range(2)]
     copy_stream = torch.cuda.Stream()
-    e2e_steps = 0 if args.no_e2e else max(3, min(args.steps, 10))
+    e2e_steps = 0 if args.no_e2e else max(3, args.steps)
     nh_total = 0
 
     def run_e2e(nsteps):
@@ -509,6 +509,18 @@ def main():
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0, world, dev)
     e2e_value = replica_value(NF * NR, e2e_steps, world, e2e_s) if e2e_steps else None
+    # the bound of the end-to-end leg: a plain pinned host -> device copy of one spectrogram
+    h2d_gbs = None
+    if e2e_steps:
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(copy_stream):
+            dev_in[0].t().copy_(pinned[0], non_blocking=True)
+            ev0.record(copy_stream)
+            for i in range(5):
+                dev_in[i % 2].t().copy_(pinned[i % nbuf], non_blocking=True)
+            ev1.record(copy_stream)
+        torch.cuda.synchronize()
+        h2d_gbs = 5 * 4 * NF * NT / (ev0.elapsed_time(ev1) * 1e-3) / 1e9
 
     # ---------------- roofline of the ZDT call ----------------
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -554,6 +566,10 @@ def main():
             "e2e": {"value": e2e_value, "unit": "cells/s",
                     "h2d_bytes_per_step": 4 * NF * NT,
                     "d2h_bytes_per_step": int(16 * nh_total / max(1, e2e_steps)) + 8,
+                    "steps": e2e_steps,
+                    "h2d_copy_gbs": h2d_gbs,
+                    "h2d_bound_cells_per_s": (NF * NR / (4 * NF * NT / (h2d_gbs * 1e9))
+                                              if h2d_gbs else None),
                     "path": "pinned host spectrogram -> device (double-buffered copy stream) -> "
                             "zdtfdr! with fused findprotohits(snr=10) -> hits to host"},
             "gpu_launches": int(launches),

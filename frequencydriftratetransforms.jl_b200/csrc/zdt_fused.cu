@@ -127,6 +127,103 @@ zdtf_input_kernel(const float* __restrict__ spec, long long N, int Nt, int Q,
   }
 }
 
+// Kernel A for P = 2048 = 64 x 32: two register passes with one shared-memory transpose (the
+// forward-sign mirror of zdtf_output_tma64_kernel).  nb = nb1 + 64*nb2, k1 = k1b + 32*k1a:
+//   X[k1b + 32 k1a] = sum_nb1 w64^(k1a nb1) [w^(k1b nb1) sum_nb2 x[nb1 + 64 nb2] w32^(k1b nb2)]
+// with w = exp(-2 pi i / P).  Thread (seq, nb1) loads its 32 values of the two packed time
+// steps straight from the spectrogram and transforms them over nb2; lanes h and h + 16 then
+// share the 64-point DFT over nb1 (decimation in time: lane h takes nb1 = 2k + h, lane 1
+// applies w64^n, one shuffle exchange), and A is stored with the inter-pass twiddle
+// exp(-2 pi i k1 n_a / Nf) from a two-level table in shared memory.  Shared-memory strides
+// as in the output kernel (S1 = 33, SSEQ = 2 mod 16): conflict-free transposes.
+struct In64Shape {
+  static constexpr int P1 = 64, P2 = 32, P = P1 * P2, TS = 8, T = 64 * TS;
+  static constexpr int S1 = P2 + 1;
+  static constexpr int SSEQ = ((P1 * S1 + 15) / 16) * 16 + 16 / TS;
+  static constexpr size_t REGION = sizeof(float2) * TS * SSEQ;
+  static constexpr size_t smem(int B, long long N) {
+    return REGION + sizeof(float2) * (P + (1LL << B) + (N >> B));
+  }
+};
+
+__global__ void __launch_bounds__(In64Shape::T, 1)
+zdtf_input64_kernel(const float* __restrict__ spec, long long N, int Nt, int Q,
+                    float2* __restrict__ A, FusedTables tab) {
+  using SH = In64Shape;
+  constexpr int P = SH::P, P1 = SH::P1, P2 = SH::P2, TS = SH::TS, S1 = SH::S1, SSEQ = SH::SSEQ;
+  extern __shared__ float2 sm[];
+  float2* region = sm;           // TS * SSEQ: the transpose
+  float2* roots = sm + TS * SSEQ;  // exp(-2 pi i m / P), m < P
+  const int nlo = 1 << tab.B, nhi = (int)(N >> tab.B);
+  float2* tlo = roots + P;  // exp(-2 pi i m / N), m < 2^B
+  float2* thi = tlo + nlo;  // exp(-2 pi i m 2^B / N), m < N / 2^B
+  const int tid = threadIdx.x;
+  for (int i = tid; i < P; i += SH::T) roots[i] = __ldg(tab.rootsP + i);
+  for (int i = tid; i < nlo; i += SH::T) tlo[i] = __ldg(tab.tw_lo + i);
+  for (int i = tid; i < nhi; i += SH::T) thi[i] = __ldg(tab.tw_hi + i);
+  const int na0 = blockIdx.x * TS;
+  const int p = blockIdx.y;
+  const float* c0 = spec + (long long)(2 * p) * N;
+  const bool has1 = (2 * p + 1) < Nt;
+  const float* c1 = spec + (long long)(2 * p + 1) * N;
+  // pass 1: thread (seq, nb1), all 32 loads of each column issued before any is used
+  const int seq1 = tid % TS, nb1 = tid / TS;
+  float2 v[P2];
+  {
+    const long long n0 = (long long)(na0 + seq1) + (long long)Q * nb1;
+    const long long st = (long long)Q * P1;
+#pragma unroll
+    for (int m = 0; m < P2; ++m) v[m].x = __ldcs(c0 + n0 + st * m);
+#pragma unroll
+    for (int m = 0; m < P2; ++m) v[m].y = has1 ? __ldcs(c1 + n0 + st * m) : 0.f;
+  }
+  __syncthreads();  // the tables are in shared memory
+  Dft<P2>::run(v, -1);
+  {
+    float2* b = region + seq1 * SSEQ + nb1 * S1;
+#pragma unroll
+    for (int k = 0; k < P2; ++k) b[k] = cmul(v[k], roots[(nb1 * k) & (P - 1)]);
+  }
+  __syncthreads();
+  // pass 2: lane = seq + TS * (k1b mod (16 / TS)) + 16 * h
+  const int lane = tid & 31;
+  const int seq2 = lane % TS, h = lane >> 4;
+  const int k1b = ((lane / TS) % (16 / TS)) + (16 / TS) * (tid >> 5);
+  {
+    const float2* b = region + seq2 * SSEQ + h * S1 + k1b;
+#pragma unroll
+    for (int k = 0; k < P1 / 2; ++k) v[k] = b[2 * k * S1];
+  }
+  Dft<P1 / 2>::run(v, -1);  // E (h = 0) or O (h = 1) at n mod 32
+  if (h) {
+#pragma unroll
+    for (int n = 1; n < P1 / 2; ++n) v[n] = cmul(v[n], roots[n * (P / P1)]);  // exp(-2 pi i n / 64)
+  }
+  // lane 0-half keeps E[0..15] and receives w O[0..15]; lane 1-half keeps w O[16..31] and
+  // receives E[16..31]: X[n] = E[n] + w^n O[n], X[n + 32] = E[n] - w^n O[n]
+#pragma unroll
+  for (int i = 0; i < P1 / 4; ++i) {
+    const float2 s = h ? v[i] : v[i + P1 / 4];
+    float2 o;
+    o.x = __shfl_xor_sync(0xffffffffu, s.x, 16);
+    o.y = __shfl_xor_sync(0xffffffffu, s.y, 16);
+    const float2 e = h ? o : v[i];
+    const float2 w = h ? v[i + P1 / 4] : o;
+    v[i] = cadd(e, w);           // k1a = i + 16h
+    v[i + P1 / 4] = csub(e, w);  // k1a = i + 16h + 32
+  }
+  const int na = na0 + seq2;
+  float2* a0 = A + (long long)p * P * Q + na;
+#pragma unroll
+  for (int i = 0; i < P1 / 2; ++i) {
+    const int k1a = (i & (P1 / 4 - 1)) + 16 * h + (i >= P1 / 4 ? P1 / 2 : 0);
+    const int k1 = k1b + P2 * k1a;
+    const long long m = (long long)k1 * na;
+    const float2 t = cmul(thi[m >> tab.B], tlo[m & (nlo - 1)]);
+    a0[(long long)k1 * Q] = cmul(v[i], t);
+  }
+}
+
 // ------------------------------------------------------------------------------------
 // Kernel B helpers
 // ------------------------------------------------------------------------------------
@@ -352,17 +449,22 @@ __global__ void __launch_bounds__(Q / 2, (Q <= 512 ? 2 : 1)) zdtf_czt_kernel(Czt
         W0y = pk_fma(Wbx, PWy[kHorner], pk_mul(Wby, PWx[kHorner]));
       }
       const float2 NW0y = pk_neg(W0y);
+      if (jh < a.Nr) {
 #pragma unroll
-      for (int jr = 0; jr < kHorner; ++jr) {
-        const float2 wx = pk_fma(W0x, PWx[jr], pk_mul(NW0y, PWy[jr]));
-        const float2 wy = pk_fma(W0x, PWy[jr], pk_mul(W0y, PWx[jr]));
-        float2 sx, sy;
-        horner_pk<NTR>(Gx, Gy, wx, wy, sx, sy);
-        sx = pk_mul(sx, WIN);
-        sy = pk_mul(sy, WIN);
-        const bool live = jh + jr < a.Nr;
-        S[0][jr] = live ? make_float2(sx.x, sy.x) : make_float2(0.f, 0.f);
-        S[1][jr] = live ? make_float2(sx.y, sy.y) : make_float2(0.f, 0.f);
+        for (int jr = 0; jr < kHorner; ++jr) {
+          const float2 wx = pk_fma(W0x, PWx[jr], pk_mul(NW0y, PWy[jr]));
+          const float2 wy = pk_fma(W0x, PWy[jr], pk_mul(W0y, PWx[jr]));
+          float2 sx, sy;
+          horner_pk<NTR>(Gx, Gy, wx, wy, sx, sy);
+          sx = pk_mul(sx, WIN);
+          sy = pk_mul(sy, WIN);
+          const bool live = jh + jr < a.Nr;
+          S[0][jr] = live ? make_float2(sx.x, sy.x) : make_float2(0.f, 0.f);
+          S[1][jr] = live ? make_float2(sx.y, sy.y) : make_float2(0.f, 0.f);
+        }
+      } else {  // a half block past the last rate (uniform over the CTA): no sums
+#pragma unroll
+        for (int jr = 0; jr < kHorner; ++jr) S[0][jr] = S[1][jr] = make_float2(0.f, 0.f);
       }
 #pragma unroll
       for (int b = 0; b < 2; ++b) {
@@ -1551,6 +1653,9 @@ static int set_smem_attrs() {
                                 (int)OutTmaShape<32, 32, 8>::SMEM));
   FDR_CUDA(cudaFuncSetAttribute(zdtf_output_tma64_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)OutTma64Shape<8>::SMEM));
+  // P = 2048 input: Nf = 2^20 or 2^21, table split B = 10 or 11
+  FDR_CUDA(cudaFuncSetAttribute(zdtf_input64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)In64Shape::smem(11, 1LL << 21)));
 #define SET_B(Q)                                                                               \
   FDR_CUDA(cudaFuncSetAttribute(zdtf_czt_kernel<Q, kFusedMaxNt>,                               \
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CztShape<Q>::SMEM)); \
@@ -1628,6 +1733,12 @@ int64_t fused_W_elems(const FusedPlan* st) { return st->N * st->npairs; }
 
 int fused_input(const FusedPlan* st, const float* spec, float2* A, cudaStream_t s) {
   const int P = st->P, Q = st->Q;
+  if (P == 2048 && Q >= In64Shape::TS) {
+    zdtf_input64_kernel<<<dim3(Q / In64Shape::TS, (unsigned)st->NP), In64Shape::T,
+                          In64Shape::smem(st->B, st->N), s>>>(spec, st->N, (int)st->Nt, Q, A, st->tab);
+    FDR_LAUNCH_CHECK("zdtf_input64_kernel");
+    return FDR_OK;
+  }
 #define LAUNCH_A(PP)                                                                           \
   if (P == PP) {                                                                               \
     constexpr int TA = AcShape<PP>::TILE, T = AcShape<PP>::T;                                  \
