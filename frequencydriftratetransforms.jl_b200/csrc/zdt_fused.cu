@@ -141,8 +141,9 @@ struct In64Shape {
   static constexpr int S1 = P2 + 1;
   static constexpr int SSEQ = ((P1 * S1 + 15) / 16) * 16 + 16 / TS;
   static constexpr size_t REGION = sizeof(float2) * TS * SSEQ;
+  static constexpr int TW1 = P1 * S1;  // tw1[nb1][k] = w^(nb1 k), rows S1 apart
   static constexpr size_t smem(int B, long long N) {
-    return REGION + sizeof(float2) * (P + (1LL << B) + (N >> B));
+    return REGION + sizeof(float2) * (TW1 + P1 / 2 + (1LL << B) + (N >> B));
   }
 };
 
@@ -153,12 +154,15 @@ zdtf_input64_kernel(const float* __restrict__ spec, long long N, int Nt, int Q,
   constexpr int P = SH::P, P1 = SH::P1, P2 = SH::P2, TS = SH::TS, S1 = SH::S1, SSEQ = SH::SSEQ;
   extern __shared__ float2 sm[];
   float2* region = sm;           // TS * SSEQ: the transpose
-  float2* roots = sm + TS * SSEQ;  // exp(-2 pi i m / P), m < P
+  float2* tw1 = sm + TS * SSEQ;  // w^(nb1 k): P1 rows of S1
+  float2* tw2 = tw1 + SH::TW1;   // w64^n, n < P1 / 2
   const int nlo = 1 << tab.B, nhi = (int)(N >> tab.B);
-  float2* tlo = roots + P;  // exp(-2 pi i m / N), m < 2^B
-  float2* thi = tlo + nlo;  // exp(-2 pi i m 2^B / N), m < N / 2^B
+  float2* tlo = tw2 + P1 / 2;  // exp(-2 pi i m / N), m < 2^B
+  float2* thi = tlo + nlo;     // exp(-2 pi i m 2^B / N), m < N / 2^B
   const int tid = threadIdx.x;
-  for (int i = tid; i < P; i += SH::T) roots[i] = __ldg(tab.rootsP + i);
+  for (int i = tid; i < P; i += SH::T)
+    tw1[(i / P2) * S1 + i % P2] = __ldg(tab.rootsP + (((i / P2) * (i % P2)) & (P - 1)));
+  for (int i = tid; i < P1 / 2; i += SH::T) tw2[i] = __ldg(tab.rootsP + i * (P / P1));
   for (int i = tid; i < nlo; i += SH::T) tlo[i] = __ldg(tab.tw_lo + i);
   for (int i = tid; i < nhi; i += SH::T) thi[i] = __ldg(tab.tw_hi + i);
   const int na0 = blockIdx.x * TS;
@@ -181,8 +185,9 @@ zdtf_input64_kernel(const float* __restrict__ spec, long long N, int Nt, int Q,
   Dft<P2>::run(v, -1);
   {
     float2* b = region + seq1 * SSEQ + nb1 * S1;
+    const float2* t1 = tw1 + nb1 * S1;
 #pragma unroll
-    for (int k = 0; k < P2; ++k) b[k] = cmul(v[k], roots[(nb1 * k) & (P - 1)]);
+    for (int k = 0; k < P2; ++k) b[k] = cmul(v[k], t1[k]);
   }
   __syncthreads();
   // pass 2: lane = seq + TS * (k1b mod (16 / TS)) + 16 * h
@@ -195,12 +200,9 @@ zdtf_input64_kernel(const float* __restrict__ spec, long long N, int Nt, int Q,
     for (int k = 0; k < P1 / 2; ++k) v[k] = b[2 * k * S1];
   }
   Dft<P1 / 2>::run(v, -1);  // E (h = 0) or O (h = 1) at n mod 32
-  if (h) {
-#pragma unroll
-    for (int n = 1; n < P1 / 2; ++n) v[n] = cmul(v[n], roots[n * (P / P1)]);  // exp(-2 pi i n / 64)
-  }
-  // lane 0-half keeps E[0..15] and receives w O[0..15]; lane 1-half keeps w O[16..31] and
-  // receives E[16..31]: X[n] = E[n] + w^n O[n], X[n + 32] = E[n] - w^n O[n]
+  // lane 0-half keeps E[0..15] and receives O[0..15]; lane 1-half keeps O[16..31] and
+  // receives E[16..31]; each applies w64^n to its 16 O values:
+  // X[n] = E[n] + w64^n O[n], X[n + 32] = E[n] - w64^n O[n]
 #pragma unroll
   for (int i = 0; i < P1 / 4; ++i) {
     const float2 s = h ? v[i] : v[i + P1 / 4];
@@ -208,7 +210,7 @@ zdtf_input64_kernel(const float* __restrict__ spec, long long N, int Nt, int Q,
     o.x = __shfl_xor_sync(0xffffffffu, s.x, 16);
     o.y = __shfl_xor_sync(0xffffffffu, s.y, 16);
     const float2 e = h ? o : v[i];
-    const float2 w = h ? v[i + P1 / 4] : o;
+    const float2 w = cmul(h ? v[i + P1 / 4] : o, tw2[i + (P1 / 4) * h]);
     v[i] = cadd(e, w);           // k1a = i + 16h
     v[i + P1 / 4] = csub(e, w);  // k1a = i + 16h + 32
   }
@@ -1138,7 +1140,10 @@ struct OutTma64Shape {
   static constexpr int NBOX = P / BOXR;
   static constexpr unsigned TILEB = sizeof(float2) * P * TS;
   static constexpr size_t REGION = sizeof(float2) * TS * SSEQ > TILEB ? sizeof(float2) * TS * SSEQ : TILEB;
-  static constexpr size_t SMEM = 128 + ((REGION + 127) / 128) * 128 + sizeof(float2) * P + 16;
+  // tables: tw1[k1a][n] = conj w^(k1a n) (pass 1: one row per thread, rows S1 apart so the
+  // two rows a half-warp reads sit in different banks), tw2[n] = conj w64^n
+  static constexpr int TW1 = P1 * S1;
+  static constexpr size_t SMEM = 128 + ((REGION + 127) / 128) * 128 + sizeof(float2) * (TW1 + P1 / 2) + 16;
   static constexpr int MINB = TS <= 4 ? 2 : 1;
 };
 
@@ -1152,8 +1157,9 @@ zdtf_output_tma64_kernel(const __grid_constant__ CUtensorMap wmap, long long N, 
   extern __shared__ unsigned char smraw[];
   const uintptr_t base = ((uintptr_t)smraw + 127) & ~(uintptr_t)127;
   float2* region = (float2*)base;
-  float2* roots = (float2*)(base + ((SH::REGION + 127) / 128) * 128);
-  unsigned long long* bar = (unsigned long long*)(roots + P);
+  float2* tw1 = (float2*)(base + ((SH::REGION + 127) / 128) * 128);  // P1 rows of S1
+  float2* tw2 = tw1 + SH::TW1;                                          // P1 / 2
+  unsigned long long* bar = (unsigned long long*)(tw2 + P1 / 2);
   const int tid = threadIdx.x;
   const int ntna = Q / TS;
   const long long ntiles = (long long)ntna * npairs;
@@ -1161,7 +1167,9 @@ zdtf_output_tma64_kernel(const __grid_constant__ CUtensorMap wmap, long long N, 
     mbar_init(&bar[0], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  for (int i = tid; i < P; i += SH::T) roots[i] = __ldg(rootsP + i);
+  for (int i = tid; i < P; i += SH::T)
+    tw1[(i / P2) * S1 + i % P2] = cconj(__ldg(rootsP + (((i / P2) * (i % P2)) & (P - 1))));
+  for (int i = tid; i < P1 / 2; i += SH::T) tw2[i] = cconj(__ldg(rootsP + i * (P / P1)));
   __syncthreads();
   auto issue = [&](long long tile) {  // thread 0 only
     const int q = (int)(tile / ntna), nat = (int)(tile - (long long)q * ntna);
@@ -1194,11 +1202,9 @@ zdtf_output_tma64_kernel(const __grid_constant__ CUtensorMap wmap, long long N, 
     Dft<P2>::run(v, +1);
     {
       float2* b = region + seq1 * SSEQ + r * S1;
+      const float2* t1 = tw1 + r * S1;
 #pragma unroll
-      for (int n = 0; n < P2; ++n) {
-        const float2 t = roots[(r * n) & (P - 1)];
-        b[n] = cmul(v[n], make_float2(t.x, -t.y));
-      }
+      for (int n = 0; n < P2; ++n) b[n] = cmul(v[n], t1[n]);
     }
     __syncthreads();
     {
@@ -1212,15 +1218,9 @@ zdtf_output_tma64_kernel(const __grid_constant__ CUtensorMap wmap, long long N, 
       issue(tile + stride);
     }
     Dft<P1 / 2>::run(v, +1);  // E (h = 0) or O (h = 1) at n mod 32
-    if (h) {
-#pragma unroll
-      for (int n = 1; n < P1 / 2; ++n) {
-        const float2 t = roots[n * (P / P1)];  // exp(-2 pi i n / 64)
-        v[n] = cmul(v[n], make_float2(t.x, -t.y));
-      }
-    }
-    // lane 0-half keeps E[0..15] and receives w O[0..15]; lane 1-half keeps w O[16..31] and
-    // receives E[16..31]: z[n] = E[n] + w^n O[n], z[n + 32] = E[n] - w^n O[n]
+    // lane 0-half keeps E[0..15] and receives O[0..15]; lane 1-half keeps O[16..31] and
+    // receives E[16..31]; each applies w^n to its 16 O values:
+    // z[n] = E[n] + w^n O[n], z[n + 32] = E[n] - w^n O[n]
 #pragma unroll
     for (int i = 0; i < P1 / 4; ++i) {
       const float2 s = h ? v[i] : v[i + P1 / 4];
@@ -1228,7 +1228,7 @@ zdtf_output_tma64_kernel(const __grid_constant__ CUtensorMap wmap, long long N, 
       o.x = __shfl_xor_sync(0xffffffffu, s.x, 16);
       o.y = __shfl_xor_sync(0xffffffffu, s.y, 16);
       const float2 e = h ? o : v[i];
-      const float2 w = h ? v[i + P1 / 4] : o;
+      const float2 w = cmul(h ? v[i + P1 / 4] : o, tw2[i + (P1 / 4) * h]);
       v[i] = cadd(e, w);             // z[i + 16h]
       v[i + P1 / 4] = csub(e, w);    // z[i + 16h + 32]
     }
