@@ -225,7 +225,6 @@ zdtf_input64_kernel(const float* __restrict__ spec, long long N, int Nt, int Q,
     a0[(long long)k1 * Q] = cmul(v[i], t);
   }
 }
-
 // ------------------------------------------------------------------------------------
 // Kernel B helpers
 // ------------------------------------------------------------------------------------
@@ -983,6 +982,17 @@ __global__ void bounded_wait_selftest_kernel(unsigned long long limit_ns) {
   const bool ok = mbar_wait_bounded(&bar, 0u, limit_ns);
   if (__syncthreads_or(!ok) && threadIdx.x == 0) atomicOr(&g_fused_fault, 8);
 }
+// FDR store of one row of a rate pair through lane pairs: v = (rate j, rate j + 1) values of
+// this lane's channel; lanes 2s and 2s + 1 hold adjacent channels, so the even lane writes
+// both channels of rate j and the odd lane both of rate j + 1 as one 8-byte streaming store
+// each (half the store instructions of per-lane scalar stores).  Every lane of the warp
+// must call it; d0 is this lane's element of rate j, d1 = d0 + Nf.
+__device__ __forceinline__ void store_rate_pair(float* d0, float* d1, float2 v, bool odd, bool has1) {
+  const float recv = __shfl_xor_sync(0xffffffffu, odd ? v.x : v.y, 1);
+  if (!odd) __stcs(reinterpret_cast<float2*>(d0), make_float2(v.x, recv));
+  else if (has1) __stcs(reinterpret_cast<float2*>(d1 - 1), make_float2(recv, v.y));
+}
+
 // 2-D tiled TMA load (no multicast) of box {x .. x+15 floats, y .. y+255 rows} into dst.
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y,
                                             unsigned long long* bar) {
@@ -1081,6 +1091,7 @@ zdtf_output_tma_kernel(const __grid_constant__ CUtensorMap wmap, long long N, in
       issue(tile + stride);
     }
     double m[4] = {0.0, 0.0, 0.0, 0.0};
+    static_assert(SH::T == TS * P2 && TS % 2 == 0, "every lane stores, channel pairs in lane pairs");
     if (r < P2) {
       Dft<P1>::run(w, +1);
       float* d0 = dest + (long long)j * N + na0 + seq + (long long)Q * r;
@@ -1088,8 +1099,7 @@ zdtf_output_tma_kernel(const __grid_constant__ CUtensorMap wmap, long long N, in
 #pragma unroll
       for (int nba = 0; nba < P1; ++nba) {
         const long long off = (long long)Q * P2 * nba;
-        __stcs(d0 + off, w[nba].x);
-        if (has1) __stcs(d1 + off, w[nba].y);
+        store_rate_pair(d0 + off, d1 + off, w[nba], seq & 1, has1);
       }
       if (acc) {
 #pragma unroll
@@ -1242,8 +1252,7 @@ zdtf_output_tma64_kernel(const __grid_constant__ CUtensorMap wmap, long long N, 
       for (int i = 0; i < P1 / 2; ++i) {
         const int nba = (i & (P1 / 4 - 1)) + 16 * h + (i >= P1 / 4 ? P1 / 2 : 0);
         const long long off = (long long)Q * P2 * nba;
-        __stcs(d0 + off, v[i].x);
-        if (has1) __stcs(d1 + off, v[i].y);
+        store_rate_pair(d0 + off, d1 + off, v[i], seq2 & 1, has1);
       }
       if (acc) {
 #pragma unroll
