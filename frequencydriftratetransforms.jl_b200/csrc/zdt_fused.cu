@@ -372,6 +372,8 @@ __global__ void __launch_bounds__(Q / 2, (Q <= 512 ? 2 : 1)) zdtf_czt_kernel(Czt
   float2* twr = twt + tw_size(Q);             // 2 * Q
   float2* gnyq = twr + 2 * Q;                 // NTR
   float2* buf2 = gnyq + NTR;                  // kRatesPerBlock * SS
+  // the thread's phase residues alpha_b, beta_b (kept in shared memory, not registers)
+  unsigned long long* phs = reinterpret_cast<unsigned long long*>(buf2 + kRatesPerBlock * SS);
   const int tid = threadIdx.x;
   const int c = blockIdx.x;
   const int P = a.P;
@@ -396,25 +398,25 @@ __global__ void __launch_bounds__(Q / 2, (Q <= 512 ? 2 : 1)) zdtf_czt_kernel(Czt
   // Per-base phase state: w_{k,j} = exp(2 pi i (alpha + j*beta) / 2^bits); rates are taken
   // kHorner at a time, w = w(first rate of the group, exact) * pw[jr] (exact).
   const unsigned long long mask = a.ph.mask;
-  unsigned long long alpha[2], beta[2];
-  float2 PWx[kHorner + 1], PWy[kHorner + 1];  // exact w(k_b, i*dr), lanes = b
+  // PWx/PWy[i - 1] = exact w(k_b, i*dr) for i = 1..kHorner (lanes = b; w(k_b, 0) = 1)
+  float2 PWx[kHorner], PWy[kHorner];
   float2 WIN;
 #pragma unroll
   for (int b = 0; b < 2; ++b) {
     const unsigned long long k = (unsigned long long)k1s[b] + (unsigned long long)P * tid;
-    alpha[b] = (k * a.ph.R0) & mask;
-    beta[b] = (k * a.ph.Rd) & mask;
+    const unsigned long long beta = (k * a.ph.Rd) & mask;
+    phs[(2 * b) * T + tid] = (k * a.ph.R0) & mask;
+    phs[(2 * b + 1) * T + tid] = beta;
 #pragma unroll
-    for (int i = 0; i <= kHorner; ++i) {
-      const float2 p = cis_phase(((unsigned long long)i * beta[b]) & mask, a.ph);
-      if (b == 0) { PWx[i].x = p.x; PWy[i].x = p.y; } else { PWx[i].y = p.x; PWy[i].y = p.y; }
+    for (int i = 1; i <= kHorner; ++i) {
+      const float2 p = cis_phase(((unsigned long long)i * beta) & mask, a.ph);
+      if (b == 0) { PWx[i - 1].x = p.x; PWy[i - 1].x = p.y; } else { PWx[i - 1].y = p.x; PWy[i - 1].y = p.y; }
     }
     const float wv = window_value(a, (long long)k);
     if (b == 0) WIN.x = wv; else WIN.y = wv;
   }
   // Nyquist bin (CTA 0, thread 0)
   const unsigned long long kny = (unsigned long long)(a.N / 2);
-  const unsigned long long alpha_n = (kny * a.ph.R0) & mask, beta_n = (kny * a.ph.Rd) & mask;
 
   int ms[2], mk2[2];
 #pragma unroll
@@ -435,8 +437,8 @@ __global__ void __launch_bounds__(Q / 2, (Q <= 512 ? 2 : 1)) zdtf_czt_kernel(Czt
     // exact phase of the block's first rate; the second half starts at w0 * w(k, 4*dr)
     float2 Wbx, Wby;
     {
-      const float2 w0 = cis_phase((alpha[0] + (unsigned long long)jg * beta[0]) & mask, a.ph);
-      const float2 w1 = cis_phase((alpha[1] + (unsigned long long)jg * beta[1]) & mask, a.ph);
+      const float2 w0 = cis_phase((phs[tid] + (unsigned long long)jg * phs[T + tid]) & mask, a.ph);
+      const float2 w1 = cis_phase((phs[2 * T + tid] + (unsigned long long)jg * phs[3 * T + tid]) & mask, a.ph);
       Wbx = make_float2(w0.x, w1.x);
       Wby = make_float2(w0.y, w1.y);
     }
@@ -446,22 +448,29 @@ __global__ void __launch_bounds__(Q / 2, (Q <= 512 ? 2 : 1)) zdtf_czt_kernel(Czt
       float2 S[2][kHorner];
       float2 W0x = Wbx, W0y = Wby;
       if (h > 0) {  // w(first rate of the half) = wb * w(k, kHorner*dr)
-        W0x = pk_fma(Wbx, PWx[kHorner], pk_mul(pk_neg(Wby), PWy[kHorner]));
-        W0y = pk_fma(Wbx, PWy[kHorner], pk_mul(Wby, PWx[kHorner]));
+        W0x = pk_fma(Wbx, PWx[kHorner - 1], pk_mul(pk_neg(Wby), PWy[kHorner - 1]));
+        W0y = pk_fma(Wbx, PWy[kHorner - 1], pk_mul(Wby, PWx[kHorner - 1]));
       }
       const float2 NW0y = pk_neg(W0y);
       if (jh < a.Nr) {
 #pragma unroll
         for (int jr = 0; jr < kHorner; ++jr) {
-          const float2 wx = pk_fma(W0x, PWx[jr], pk_mul(NW0y, PWy[jr]));
-          const float2 wy = pk_fma(W0x, PWy[jr], pk_mul(W0y, PWx[jr]));
+          float2 wx = W0x, wy = W0y;  // jr = 0: w(k, 0) = 1
+          if (jr > 0) {
+            wx = pk_fma(W0x, PWx[jr - 1], pk_mul(NW0y, PWy[jr - 1]));
+            wy = pk_fma(W0x, PWy[jr - 1], pk_mul(W0y, PWx[jr - 1]));
+          }
           float2 sx, sy;
           horner_pk<NTR>(Gx, Gy, wx, wy, sx, sy);
           sx = pk_mul(sx, WIN);
           sy = pk_mul(sy, WIN);
-          const bool live = jh + jr < a.Nr;
-          S[0][jr] = live ? make_float2(sx.x, sy.x) : make_float2(0.f, 0.f);
-          S[1][jr] = live ? make_float2(sx.y, sy.y) : make_float2(0.f, 0.f);
+          S[0][jr] = make_float2(sx.x, sy.x);
+          S[1][jr] = make_float2(sx.y, sy.y);
+        }
+        if (jh + kHorner > a.Nr) {  // rates past the grid's last (uniform over the CTA): zero
+#pragma unroll
+          for (int jr = 0; jr < kHorner; ++jr)
+            if (jh + jr >= a.Nr) S[0][jr] = S[1][jr] = make_float2(0.f, 0.f);
         }
       } else {  // a half block past the last rate (uniform over the CTA): no sums
 #pragma unroll
@@ -492,6 +501,7 @@ __global__ void __launch_bounds__(Q / 2, (Q <= 512 ? 2 : 1)) zdtf_czt_kernel(Czt
 #pragma unroll
         for (int hh = 0; hh < 2; ++hh) {
           const int j = j0 + 2 * u + hh;
+          const unsigned long long alpha_n = (kny * a.ph.R0) & mask, beta_n = (kny * a.ph.Rd) & mask;
           const float2 w = cis_phase((alpha_n + (unsigned long long)(jg + 2 * u + hh) * beta_n) & mask, a.ph);
           const float2 sv = horner<NTR>(Gn, w);
           v[hh] = (j < a.Nr) ? sv.x * wn : 0.f;  // real-only Nyquist bin
@@ -1533,9 +1543,10 @@ struct AcShape {
 };
 
 template <int Q>
-struct CztShape {  // buf | twt | twr | gnyq | buf2 (the second rate-block buffer)
+struct CztShape {  // buf | twt | twr | gnyq | buf2 (the second rate-block buffer) | phase residues
   static constexpr size_t SMEM =
-      sizeof(float2) * (2 * kRatesPerBlock * b_stride<Q>() + tw_size(Q) + 2 * Q + kFusedMaxNt);
+      sizeof(float2) * (2 * kRatesPerBlock * b_stride<Q>() + tw_size(Q) + 2 * Q + kFusedMaxNt) +
+      sizeof(unsigned long long) * 4 * (Q / 2);
 };
 
 // log2 of the four-step factor Q for Nf = 2^L and Nt time steps.  With F in registers

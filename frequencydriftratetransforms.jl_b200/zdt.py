@@ -44,8 +44,9 @@ class ZDTWorkspace:
     ``shape``.  Extra keyword flags: ``exact_phase`` (reduce chirp phases exactly instead
     of reproducing the reference's Float32 arguments in the staged stages),
     ``staged_only`` (zdtfdr_ always runs the staged kernels) and ``mixed_precision`` (the
-    fused output pass, for P = 1024 shapes such as Nf = 2^20 with Nt <= 16, runs its DFTs
-    as split-bfloat16 tensor-core contractions: ~1e-5 relative error instead of ~1e-6).
+    fused output pass runs its DFTs as split-bfloat16 tensor-core contractions where the
+    four-step split has P = 1024: Nf = 2^19 and, since such a workspace splits Nf = 2^20 as
+    1024 x 1024, Nf = 2^20 with Nt <= 16; ~1e-5 relative error instead of ~1e-6).
     """
 
     def __init__(self, spectrogram, r0_or_rates, dr=None, Nr=None, factors=(2, 3, 5), *,
