@@ -82,7 +82,7 @@ def algorithmic_bytes():
 
 # DRAM bytes (read + write) of one fused zdtfdr! call at this workload, summed over its three
 # kernels from one ncu capture (profiles/zdt_kernels_traffic_Nf2e20_Nt16_Nr129.md).
-NCU_TRAFFIC_PER_CALL = 1_687_522_816
+NCU_TRAFFIC_PER_CALL = 1_676_704_256
 
 
 def nominal_flops():
