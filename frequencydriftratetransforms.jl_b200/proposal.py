@@ -214,7 +214,7 @@ def synth_channel(seed, Nf=1 << 20, Nt=16, max_tones=5, snr=(8.0, 40.0), rmax=8.
 
 class FullSearch:
     """Full-rate plain ZDT (256 rates, -8:1/16:8-1/16) + fused proto-hit scan: the labeller,
-    the low-confidence fallback and the judge of recall."""
+    the low-confidence fallback and the reference against which recall is measured."""
 
     def __init__(self, Nf=1 << 20, Nt=16):
         self.ws = ZDTWorkspace(None, R_MIN, DR, NRATES, shape=(Nf, Nt))
