@@ -50,6 +50,57 @@ intfdr_kernel(const float* __restrict__ spec, long long Nf, int Nt, int nrates,
   }
 }
 
+// Tiled form for shift sets that stay close together (every rate of a launch within a
+// window of each column): a CTA stages, per time step t, the spectrogram channels
+// [n0 + lo_t, n0 + TN + hi_t] (modulo Nf) in shared memory and forms its TN output channels
+// of every rate from there, with the same sequence of float32 additions.  Each spectrogram
+// element is then read from HBM about once per CTA instead of once per rate.
+constexpr int kTiledMaxNt = 64;
+constexpr int kTiledMaxWords = 24576;  // shared-memory window floats (96 KB)
+
+struct TiledTable {
+  int32_t rel[kShiftParamWords];  // shift of rate jj at time t, minus lo_t: rel[jj*Nt + t]
+  int32_t lo[kTiledMaxNt];        // smallest signed shift at time t (in (-Nf/2, Nf/2])
+  int32_t off[kTiledMaxNt + 1];   // start of time step t's window in shared memory
+};
+
+template <int TNV>  // TN = TNV * kIntfdrThreads output channels per CTA
+__global__ void __launch_bounds__(kIntfdrThreads)
+intfdr_tiled_kernel(const float* __restrict__ spec, long long Nf, int Nt, int nrates,
+                    float* __restrict__ fdr, const __grid_constant__ TiledTable tab) {
+  constexpr int TN = TNV * kIntfdrThreads;
+  extern __shared__ float win[];
+  const long long n0 = (long long)blockIdx.x * TN;
+  for (int t = 0; t < Nt; ++t) {
+    const float* col = spec + (long long)t * Nf;
+    const int len = tab.off[t + 1] - tab.off[t];
+    long long idx = (n0 + tab.lo[t]) % Nf;
+    if (idx < 0) idx += Nf;
+    for (int i = threadIdx.x; i < len; i += kIntfdrThreads) {
+      long long g = idx + i;
+      if (g >= Nf) g -= Nf;  // len <= TN + Nf/4 < Nf: one wrap at most
+      win[tab.off[t] + i] = __ldg(col + g);
+    }
+  }
+  __syncthreads();
+  // the TNV channels of a thread are independent sums: interleaved, each in time order
+  for (int jj = 0; jj < nrates; ++jj) {
+    float acc[TNV];
+#pragma unroll
+    for (int v = 0; v < TNV; ++v) acc[v] = 0.0f;
+    for (int t = 0; t < Nt; ++t) {
+      const float* w = win + tab.off[t] + tab.rel[jj * Nt + t] + threadIdx.x;
+#pragma unroll
+      for (int v = 0; v < TNV; ++v) acc[v] = __fadd_rn(acc[v], w[v * kIntfdrThreads]);
+    }
+#pragma unroll
+    for (int v = 0; v < TNV; ++v) {
+      const long long n = n0 + threadIdx.x + v * kIntfdrThreads;
+      if (n < Nf) fdr[(long long)jj * Nf + n] = acc[v];
+    }
+  }
+}
+
 __global__ void intshift_kernel(const float* __restrict__ din, long long Nf, int Nt,
                                 float* __restrict__ dout, const __grid_constant__ ShiftTable tab) {
   const long long total = Nf * Nt;
@@ -80,6 +131,59 @@ static int32_t mod_nf(int64_t sh, int64_t Nf) {
   return (int32_t)m;
 }
 
+// Tiled launch of rates [j0, j0 + nr) if their shifts fit the shared-memory windows;
+// false if not (the caller uses the untiled kernel).
+static bool run_intfdr_tiled(const float* spec, int64_t Nf, int64_t Nt, int64_t j0, int64_t nr,
+                             float* fdr, const std::vector<int32_t>& sh, cudaStream_t s, int* status) {
+  *status = FDR_OK;
+  if (Nt > kTiledMaxNt || nr * Nt > kShiftParamWords || Nf < 2 * kIntfdrThreads) return false;
+  TiledTable tab;
+  int64_t spans = 0;
+  for (int64_t t = 0; t < Nt; ++t) {
+    int64_t lo = 0, hi = 0;
+    for (int64_t j = 0; j < nr; ++j) {
+      int64_t v = sh[(j0 + j) * Nt + t];  // in [0, Nf)
+      if (v > Nf / 2) v -= Nf;            // signed representative in (-Nf/2, Nf/2]
+      if (j == 0 || v < lo) lo = v;
+      if (j == 0 || v > hi) hi = v;
+    }
+    if (hi - lo > Nf / 4) return false;
+    tab.lo[t] = (int32_t)lo;
+    spans += hi - lo;
+    for (int64_t j = 0; j < nr; ++j) {
+      int64_t v = sh[(j0 + j) * Nt + t];
+      if (v > Nf / 2) v -= Nf;
+      tab.rel[j * Nt + t] = (int32_t)(v - lo);
+    }
+  }
+  int TN = 0;
+  for (int tn = 1024; tn >= 256; tn /= 2)  // TN <= Nf/2 and spans <= Nf/4: windows < Nf
+    if (Nt * (int64_t)tn + spans <= kTiledMaxWords && 2 * (int64_t)tn <= Nf) { TN = tn; break; }
+  if (TN == 0) return false;
+  tab.off[0] = 0;
+  for (int64_t t = 0; t < Nt; ++t) {
+    int64_t hi = 0;
+    for (int64_t j = 0; j < nr; ++j) hi = std::max<int64_t>(hi, tab.rel[j * Nt + t]);
+    tab.off[t + 1] = tab.off[t] + (int32_t)(TN + hi);  // channels n0 + lo .. n0 + TN - 1 + hi
+  }
+  const size_t smem = sizeof(float) * (size_t)tab.off[Nt];
+  cudaError_t ea = cudaSuccess;
+#define TILED(V)                                                                                \
+  if (TN == V * kIntfdrThreads) {                                                               \
+    ea = cudaFuncSetAttribute(intfdr_tiled_kernel<V>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                              (int)(sizeof(float) * kTiledMaxWords));                           \
+    if (ea == cudaSuccess)                                                                      \
+      intfdr_tiled_kernel<V><<<(unsigned)cdiv(Nf, TN), kIntfdrThreads, smem, s>>>(             \
+          spec, Nf, (int)Nt, (int)nr, fdr + j0 * Nf, tab);                                      \
+  }
+  TILED(1) TILED(2) TILED(4)
+#undef TILED
+  if (ea != cudaSuccess) { *status = cuda_status(ea, "intfdr tiled attribute"); return true; }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) *status = cuda_status(e, "intfdr_tiled_kernel");
+  return true;
+}
+
 static int run_intfdr(const float* spec, int64_t Nf, int64_t Nt, int64_t Nr, float* fdr,
                       const std::vector<int32_t>& sh, cudaStream_t s) {
   FDR_CHECK_ARG(Nt <= kShiftParamWords, "intfdr: Nt=%lld exceeds %d", (long long)Nt,
@@ -89,6 +193,11 @@ static int run_intfdr(const float* spec, int64_t Nf, int64_t Nt, int64_t Nr, flo
   ShiftTable tab;
   for (int64_t j0 = 0; j0 < Nr; j0 += chunk) {
     const int64_t nr = std::min(chunk, Nr - j0);
+    int st = FDR_OK;
+    if (run_intfdr_tiled(spec, Nf, Nt, j0, nr, fdr, sh, s, &st)) {
+      if (st != FDR_OK) return st;
+      continue;
+    }
     memcpy(tab.sh, sh.data() + j0 * Nt, sizeof(int32_t) * nr * Nt);
     intfdr_kernel<<<gx, kIntfdrThreads, 0, s>>>(spec, Nf, (int)Nt, (int)nr, fdr + j0 * Nf, tab);
     FDR_LAUNCH_CHECK("intfdr_kernel");
