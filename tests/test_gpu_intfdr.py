@@ -61,6 +61,22 @@ def test_large_shifts_wrap(fdr, oracle):
     assert np.array_equal(bits(out), bits(ref))
 
 
+@pytest.mark.parametrize("Nf,Nt,rates", [
+    (4096, 16, [float(r) for r in range(-15, 16)]),   # shared-memory windows, wrapping at 0
+    (1024, 16, [float(r) for r in range(-15, 16)]),   # spread > Nf/4: per-element kernel
+    (8192, 80, [-2.0, -0.5, 0.25, 1.5]),              # Nt > 64: per-element kernel
+    (777, 9, [-1.5, 0.5, 2.5]),                       # ragged last tile
+])
+def test_bit_exact_tiled_and_untiled(fdr, oracle, Nf, Nt, rates):
+    """Both intfdr kernels (shared-memory windows where every rate's shift of a time step
+    lies within Nf/4 of the others, per-element gathers otherwise) give the reference's
+    float32 sums bit for bit."""
+    spec, _ = oracle.synth_spectrogram(Nf, Nt, 3, 20, 20, 4, seed=Nf + 3 * Nt)
+    out = fdr.intfdr(spec, rates).cpu().numpy()
+    ref = oracle.intfdr(spec, rates)
+    assert np.array_equal(bits(out), bits(ref))
+
+
 def test_intshift_random(fdr, oracle):
     spec, _ = oracle.synth_spectrogram(4096, 16, 2, 20, 20, 4, seed=4)
     for r in [-3.75, 0.5, 2.25, 17.0]:
