@@ -362,7 +362,8 @@ __device__ __forceinline__ float window_value(const CztArgs& a, long long k) {
 // ------------------------------------------------------------------------------------
 // Kernel B: grid (P/2, rate groups), Q/2 threads.
 // ------------------------------------------------------------------------------------
-template <int Q, int NTR>
+// WINDOWED = false: the rectangular window (weights 1, skipped: the same FDR bit for bit).
+template <int Q, int NTR, bool WINDOWED>
 __global__ void __launch_bounds__(Q / 2, (Q <= 512 ? 2 : 1)) zdtf_czt_kernel(CztArgs a) {
   constexpr int T = Q / 2;
   constexpr int SS = b_stride<Q>();
@@ -462,8 +463,10 @@ __global__ void __launch_bounds__(Q / 2, (Q <= 512 ? 2 : 1)) zdtf_czt_kernel(Czt
           }
           float2 sx, sy;
           horner_pk<NTR>(Gx, Gy, wx, wy, sx, sy);
-          sx = pk_mul(sx, WIN);
-          sy = pk_mul(sy, WIN);
+          if (WINDOWED) {
+            sx = pk_mul(sx, WIN);
+            sy = pk_mul(sy, WIN);
+          }
           S[0][jr] = make_float2(sx.x, sy.x);
           S[1][jr] = make_float2(sx.y, sy.y);
         }
@@ -1677,7 +1680,9 @@ static int set_smem_attrs() {
   FDR_CUDA(cudaFuncSetAttribute(zdtf_input64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)In64Shape::smem(11, 1LL << 21)));
 #define SET_B(Q)                                                                               \
-  FDR_CUDA(cudaFuncSetAttribute(zdtf_czt_kernel<Q, kFusedMaxNt>,                               \
+  FDR_CUDA(cudaFuncSetAttribute(zdtf_czt_kernel<Q, kFusedMaxNt, false>,                        \
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CztShape<Q>::SMEM)); \
+  FDR_CUDA(cudaFuncSetAttribute(zdtf_czt_kernel<Q, kFusedMaxNt, true>,                         \
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CztShape<Q>::SMEM)); \
   FDR_CUDA(cudaFuncSetAttribute(zdtf_a2f_kernel<Q, kFusedMaxNt>,                               \
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CztShape<Q>::SMEM));
@@ -1870,7 +1875,10 @@ int fused_czt_blocks(const FusedPlan* st, const float2* A, float2* W, float r0, 
   } else {
 #define LAUNCH_B(QQ)                                                                           \
     if (Q == QQ) {                                                                             \
-      zdtf_czt_kernel<QQ, kFusedMaxNt><<<dim3(ctas, groups), QQ / 2, CztShape<QQ>::SMEM, s>>>(a); \
+      if (window == FDR_WINDOW_RECT)                                                           \
+        zdtf_czt_kernel<QQ, kFusedMaxNt, false><<<dim3(ctas, groups), QQ / 2, CztShape<QQ>::SMEM, s>>>(a); \
+      else                                                                                     \
+        zdtf_czt_kernel<QQ, kFusedMaxNt, true><<<dim3(ctas, groups), QQ / 2, CztShape<QQ>::SMEM, s>>>(a); \
       FDR_LAUNCH_CHECK("zdtf_czt_kernel");                                                     \
       return FDR_OK;                                                                           \
     }
