@@ -15,7 +15,7 @@ from .zdtutils import calcNl, growNr, estimate_memory, driftrates
 from .batchrates import batchrates, RateRange
 from .zdt import (ZDTWorkspace, input_, preprocess_, convolve_, postprocess_, output_,
                   zdtfdr_, zdtfdr_nodest_, zdtfdr, zdtfdr_protohits_, zdtfdr_blocks_,
-                  zdtfdr_blocks_protohits_)
+                  zdtfdr_blocks_protohits_, fused_split)
 from .batch import ZDTBatch
 from . import proposal
 from . import ingest
@@ -33,7 +33,7 @@ __all__ = [
     "calcNl", "growNr", "estimate_memory", "driftrates", "batchrates", "RateRange",
     "ZDTWorkspace", "input_", "preprocess_", "convolve_", "postprocess_", "output_",
     "zdtfdr_", "zdtfdr_nodest_", "zdtfdr", "zdtfdr_protohits_", "zdtfdr_blocks_",
-    "zdtfdr_blocks_protohits_", "ZDTBatch", "proposal",
+    "zdtfdr_blocks_protohits_", "fused_split", "ZDTBatch", "proposal",
     "intshift", "intshift_", "intfdr", "intfdr_",
     "FFTFDRWorkspace", "fftfdr_workspace", "fftfdr_workspace_", "fdshiftsum", "fdshiftsum_",
     "fdshift", "fdshift_", "fftfdr", "fftfdr_",

@@ -88,6 +88,7 @@ SIGNATURES = {
                              C.c_uint32, P]),
     "fdr_zdt_destroy": (INT, [P]),
     "fdr_zdt_get_info": (INT, [P, C.POINTER(fdr_zdt_info)]),
+    "fdr_zdt_fused_split": (INT, [I64, I64, I64, C.c_uint32, C.POINTER(I64), C.POINTER(I64)]),
     "fdr_zdt_buffers": (INT, [P, C.POINTER(P), C.POINTER(P), C.POINTER(P)]),
     "fdr_zdt_input": (INT, [P, P, P]),
     "fdr_zdt_preprocess": (INT, [P, F32, P]),

@@ -347,6 +347,20 @@ int fdr_zdt_get_info(const fdr_zdt* ws, fdr_zdt_info* info) {
   return FDR_OK;
 }
 
+int fdr_zdt_fused_split(int64_t Nf, int64_t Nt, int64_t Nr, uint32_t flags, int64_t* P, int64_t* Q) {
+  FDR_CHECK_ARG(P && Q, "fdr_zdt_fused_split: NULL argument");
+  if ((flags & FDR_ZDT_STAGED_ONLY) || !zdt_fused_eligible(Nf, Nt, Nr)) {
+    set_error(FDR_ERR_UNSUPPORTED_SIZE, "fdr_zdt_fused_split: Nf=%lld Nt=%lld Nr=%lld runs the staged kernels",
+              (long long)Nf, (long long)Nt, (long long)Nr);
+    return FDR_ERR_UNSUPPORTED_SIZE;
+  }
+  int pl = 0, ql = 0;
+  fused_split_log2(Nf, Nt, (flags & FDR_ZDT_MIXED_PRECISION) != 0, &pl, &ql);
+  *P = (int64_t)1 << pl;
+  *Q = (int64_t)1 << ql;
+  return FDR_OK;
+}
+
 int fdr_zdt_buffers(fdr_zdt* ws, void** F, void** Y, void** V) {
   FDR_CHECK_ARG(ws != nullptr, "fdr_zdt_buffers: NULL workspace");
   if (F) {

@@ -1563,6 +1563,12 @@ static int fused_qlog(int L, int64_t Nt, bool p1024 = false) {
   return std::min(cap, (L + 1) / 2);
 }
 
+void fused_split_log2(int64_t Nf, int64_t Nt, bool p1024, int* Plog, int* Qlog) {
+  const int L = ilog2(Nf);
+  *Qlog = fused_qlog(L, Nt, p1024);
+  *Plog = L - *Qlog;
+}
+
 bool zdt_fused_eligible(int64_t Nf, int64_t Nt, int64_t Nr) {
   if (!is_pow2(Nf) || Nt > kFusedMaxNtSmem || Nt < 1 || Nr < 1) return false;
   const int L = ilog2(Nf);

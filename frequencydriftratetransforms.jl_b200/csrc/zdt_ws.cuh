@@ -43,6 +43,8 @@ int zdt_stage_input(fdr_zdt* ws, const float* spec, cudaStream_t s);
 int zdt_ensure_F(fdr_zdt* ws, cudaStream_t s);
 // Fused path (zdt_fused.cu)
 bool zdt_fused_eligible(int64_t Nf, int64_t Nt, int64_t Nr);
+// log2 of P and Q of the fused split (Nf a power of two, zdt_fused_eligible true).
+void fused_split_log2(int64_t Nf, int64_t Nt, bool p1024, int* Plog, int* Qlog);
 int zdt_fused_setup(fdr_zdt* ws);
 int zdt_fused_input(fdr_zdt* ws, const float* spec, cudaStream_t s);
 int zdt_fused_A_to_F(fdr_zdt* ws, cudaStream_t s);

@@ -150,6 +150,20 @@ class ZDTWorkspace:
         return [(names[i].decode(), float(times[i])) for i in range(n.value)]
 
 
+def fused_split(Nf, Nt, Nr, *, mixed_precision=False, staged_only=False):
+    """The four-step split (P, Q), Nf = P * Q, that the fused path of a workspace with these
+    sizes and flags uses (P residues in the input and output passes, Q bins per czt CTA),
+    or None when zdtfdr_ runs the staged kernels.  Host arithmetic only."""
+    flags = (_lib.FDR_ZDT_MIXED_PRECISION if mixed_precision else 0) | (
+        _lib.FDR_ZDT_STAGED_ONLY if staged_only else 0)
+    P, Q = C.c_int64(0), C.c_int64(0)
+    st = _lib.lib().fdr_zdt_fused_split(int(Nf), int(Nt), int(Nr), flags, C.byref(P), C.byref(Q))
+    if st == _lib.FDR_ERR_UNSUPPORTED_SIZE:
+        return None
+    _lib.check(st)
+    return int(P.value), int(Q.value)
+
+
 def _window_args(w, K, Nf):
     if w is None or w == "rect":
         return _lib.FDR_WINDOW_RECT, None

@@ -124,6 +124,11 @@ int fdr_zdt_create(fdr_zdt** ws, const float* spectrogram, int64_t Nf, int64_t N
 int fdr_zdt_destroy(fdr_zdt* ws);
 /* show / sizeof / driftrates (zdtfdr.jl:89-103, zdtutils.jl:62-64). */
 int fdr_zdt_get_info(const fdr_zdt* ws, fdr_zdt_info* info);
+/* No reference counterpart: the four-step split Nf = P x Q that the fused path of a
+   workspace with these sizes and flags uses (P residues in the input and output passes, Q
+   bins per czt CTA).  FDR_ERR_UNSUPPORTED_SIZE when the fused path does not apply (the
+   staged kernels run).  Host arithmetic only: touches no device. */
+int fdr_zdt_fused_split(int64_t Nf, int64_t Nt, int64_t Nr, uint32_t flags, int64_t* P, int64_t* Q);
 /* Field access to ws.F, ws.Y (Yf and Ys are its first Nt / Nr columns) and ws.V. */
 int fdr_zdt_buffers(fdr_zdt* ws, void** F, void** Y, void** V);
 /* input! (zdtfdr.jl:209-212): F = rfft(spectrogram, dims=1). */

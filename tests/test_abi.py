@@ -58,6 +58,29 @@ def test_argument_errors_without_device(fdr):
     assert st == fdr._lib.FDR_ERR_INVALID_ARGUMENT
 
 
+def test_fused_split_plan(fdr):
+    """The four-step split of the fused path, chosen on the host: 512 bins per czt CTA up to
+    Nf = 2^20 with F in registers (Nt <= 16), 1024 above and for mixed-precision workspaces
+    at 2^20 (their tensor-core output pass is written for P = 1024), 512 / 256 bins with F
+    in shared memory (Nt <= 32 / 64); the staged kernels outside 2^12..2^22 or P > 4096."""
+    fs = fdr.fused_split
+    assert fs(2 ** 20, 16, 129) == (2048, 512)
+    assert fs(2 ** 20, 16, 129, mixed_precision=True) == (1024, 1024)
+    assert fs(2 ** 19, 16, 129) == (1024, 512)
+    assert fs(2 ** 21, 16, 17) == (2048, 1024)
+    assert fs(2 ** 22, 16, 17) == (4096, 1024)
+    assert fs(2 ** 20, 24, 33) == (2048, 512)
+    assert fs(2 ** 20, 64, 65) == (4096, 256)
+    assert fs(2 ** 18, 40, 33) == (1024, 256)
+    assert fs(2 ** 12, 16, 17) == (64, 64)
+    for Nf, Nt in ((2 ** 23, 16), (2 ** 11, 16), (3 * 2 ** 18, 16), (2 ** 20, 65), (2 ** 22, 64)):
+        assert fs(Nf, Nt, 17) is None, (Nf, Nt)
+    assert fs(2 ** 20, 16, 129, staged_only=True) is None
+    for Nf, Nt in ((2 ** 16, 16), (2 ** 20, 16), (2 ** 21, 32)):
+        P, Q = fs(Nf, Nt, 33)
+        assert P * Q == Nf
+
+
 def test_batchrates_host_matches_oracle(fdr, oracle):
     for args in [(16, 1.0, -4.0, None, 360), (16, 0.5, 10.0, -3.0, 50),
                  (32, -0.25, -2.0, 5.0, 40), (17, 0.1, -100.0, 100.0, 360), (64, 1.0, -8.0, 8.0, 100)]:
