@@ -29,6 +29,10 @@ FDR_ZDT_OUTPUT_ALIGNED = 0x1
 FDR_ZDT_EXACT_PHASE = 0x2
 FDR_ZDT_STAGED_ONLY = 0x4
 FDR_ZDT_MIXED_PRECISION = 0x8
+FDR_ZDT_FAST_STATS = 0x10
+
+FDR_SNR_F64 = 1
+FDR_SNR_F32 = 2
 
 FDR_RATES_F64 = 0
 FDR_RATES_F32 = 1
@@ -175,6 +179,19 @@ def check(status: int):
         if status == FDR_ERR_CAPACITY:
             raise CapacityError(status, msg)
         raise FDRError(status, msg)
+
+
+def snr_mode(threshold, snr):
+    """The `snr` argument of the proto-hit searches for a Python threshold: 0 without snr;
+    with snr, the type Julia's promotion gives fdrdenormalize(threshold, m, s) =
+    threshold*s + m for Float32 m and s: Float32 for an integer or numpy float32 threshold
+    (FDR_SNR_F32), Float64 for a Python or numpy float64 (FDR_SNR_F64)."""
+    import numpy as np
+    if not snr:
+        return 0
+    if isinstance(threshold, (bool, int, np.integer, np.float32)):
+        return FDR_SNR_F32
+    return FDR_SNR_F64
 
 
 def i64_array(values):

@@ -119,11 +119,19 @@ int sm_count();
 // fdrutils.cu helpers shared with the ZDT driver.
 int upload_ptrs(const void* const* host, int64_t nb, void*** dev, cudaStream_t s);
 int stats_device(const float* const* d_mats, int64_t nb, int64_t Nf, int64_t Nrb, double* d_ms,
-                 cudaStream_t s);
+                 int snr_mode, double snr, cudaStream_t s);
+// Float32 fdrstats in the reference's pairwise order over nb*Nrb columns (device pointer
+// array d_mats, or the contiguous matrix `base` when d_mats is NULL).  `part` holds
+// 2*ncols*pairwise_stats_parts(Nf, ncols, smax) floats of scratch; d_ms receives m, s and
+// the threshold fdrdenormalize(snr, m, s) (snr_mode FDR_SNR_F64 / FDR_SNR_F32).
+int pairwise_stats_parts(long long Nf, long long ncols, int smax);
+int pairwise_stats_launch(const float* const* d_mats, const float* base, long long nb, long long Nf,
+                          long long Nrb, float* part, int smax, double* d_ms, int snr_mode,
+                          double snr, cudaStream_t s);
 int moments_accumulate(const float* x, long long Nf, long long ncols, double* acc, cudaStream_t s);
 int stats_finalize_launch(const double* acc, long long ncols, long long Nf, double* d_ms,
                           cudaStream_t s);
-int threshold_launch(const double* d_ms, double snr, double* d_thr, cudaStream_t s);
+int threshold_launch(const double* d_ms, int snr_mode, double snr, double* d_thr, cudaStream_t s);
 int hits_run(const float* const* d_mats, int64_t nb, int64_t Nf, int64_t Nrb, double thr_host,
              const double* d_thr, int64_t* hits, int64_t capacity, int64_t* count,
              double* thr_used, cudaStream_t s);

@@ -13,34 +13,230 @@ constexpr int kHitThreads = 256;
 constexpr int kHitRounds = 16;
 constexpr long long kHitTile = (long long)kHitThreads * kHitRounds;  // elements per tile
 
-// Per-column sum and sum of squares in float64.  grid.x: chunks of rows; grid.y: columns.
-__global__ void __launch_bounds__(kRedThreads)
-column_moments_kernel(const float* const* __restrict__ mats, long long Nf, long long Nrb,
-                      double* __restrict__ acc /* [col][2] */) {
-  const long long col = blockIdx.y;             // global column (matrix-major)
-  const long long b = col / Nrb, j = col - b * Nrb;
-  const float* x = mats[b] + j * Nf;
-  double s1 = 0.0, s2 = 0.0;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < Nf;
-       i += (long long)gridDim.x * blockDim.x) {
-    double v = (double)x[i];
-    s1 += v;
-    s2 += v * v;
+// ------------------------------------------------------------------------------------
+// fdrstats in the reference's Float32 arithmetic.
+//
+// m = mean(fdr[:,1]) and s = minimum(std(fdr, dims=1)) (fdrutils.jl:39-50) reduce each
+// column with Julia's pairwise mapreduce (Base.mapreduce_impl, block size 1024): a range of
+// at most 1024 elements (a leaf) is summed sequentially, ((f(a1) + f(a2)) + f(a3)) + ...,
+// and a longer range [lo, hi] splits at mid = lo + (hi - lo) >> 1, its value being
+// left + right.  mean = sum / Float32(n); Statistics.varm! scales the pairwise sum of
+// abs2(x - mean) by Float32(1 // (n - 1)); std = sqrt of that, all in Float32.
+//
+// With D the smallest depth at which every node of the recursion has at most 1024
+// elements (node lengths at depth d are ceil(n/2^d) or floor(n/2^d)), every node above
+// depth D-1 is internal and every node at depth D-1 (a "unit", M = 2^(D-1) of them) is one
+// leaf or two.  A unit's range follows from its index: from the root, bit b of the index
+// (most significant first) picks the left part (the first ceil(len/2) elements) or the
+// right part.  Units are summed by threads, and combined in order up a perfect binary tree:
+// within a thread (G consecutive units), across the CTA (T threads) and across the S CTAs of
+// a column (S partials, combined by the next kernel).
+// ------------------------------------------------------------------------------------
+constexpr int kPwThreads = 128;
+constexpr long long kPwLeaf = 1024;
+
+__device__ __forceinline__ const float* pw_column(const float* const* mats, const float* base,
+                                                  long long Nf, long long Nrb, long long col) {
+  if (mats) {
+    const long long b = col / Nrb;
+    return mats[b] + (col - b * Nrb) * Nf;
   }
-  __shared__ double r1[kRedThreads / 32], r2[kRedThreads / 32];
-  for (int o = 16; o > 0; o >>= 1) {
-    s1 += __shfl_down_sync(0xffffffffu, s1, o);
-    s2 += __shfl_down_sync(0xffffffffu, s2, o);
+  return base + col * Nf;
+}
+
+// f(x) of the reduction: x (sum) or abs2(x - m) (centralised sum of squares), rounded as
+// Julia's Float32 operations, never fused into a multiply-add.
+template <bool SQ>
+__device__ __forceinline__ float pw_f(float x, float m) {
+  if (SQ) {
+    const float d = __fsub_rn(x, m);
+    return __fmul_rn(d, d);
   }
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (lane == 0) { r1[w] = s1; r2[w] = s2; }
+  return x;
+}
+
+template <bool SQ>
+__device__ __forceinline__ float pw_add4(float v, float4 a, float m) {
+  v = __fadd_rn(v, pw_f<SQ>(a.x, m));
+  v = __fadd_rn(v, pw_f<SQ>(a.y, m));
+  v = __fadd_rn(v, pw_f<SQ>(a.z, m));
+  return __fadd_rn(v, pw_f<SQ>(a.w, m));
+}
+
+// Sequential sum of one leaf of len >= 1 elements.
+template <bool SQ>
+__device__ float pw_leaf(const float* __restrict__ p, long long len, float m) {
+  float v;
+  long long i;
+  if ((reinterpret_cast<uintptr_t>(p) & 15) == 0 && len >= 4) {
+    const float4* q = reinterpret_cast<const float4*>(p);
+    const long long nq = len >> 2;
+    const float4 a = __ldg(q);
+    v = pw_f<SQ>(a.x, m);
+    v = __fadd_rn(v, pw_f<SQ>(a.y, m));
+    v = __fadd_rn(v, pw_f<SQ>(a.z, m));
+    v = __fadd_rn(v, pw_f<SQ>(a.w, m));
+    long long k = 1;
+    for (; k + 8 <= nq; k += 8) {  // eight 16-byte loads in flight, then their 32 adds in order
+      float4 b[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) b[u] = __ldg(q + k + u);
+#pragma unroll
+      for (int u = 0; u < 8; ++u) v = pw_add4<SQ>(v, b[u], m);
+    }
+    for (; k < nq; ++k) v = pw_add4<SQ>(v, __ldg(q + k), m);
+    i = nq << 2;
+  } else {
+    v = pw_f<SQ>(__ldg(p), m);
+    i = 1;
+  }
+  for (; i < len; ++i) v = __fadd_rn(v, pw_f<SQ>(__ldg(p + i), m));
+  return v;
+}
+
+// Value of unit u (depth `bits` node) of a column of n elements.
+template <bool SQ>
+__device__ float pw_unit(const float* __restrict__ x, long long n, int bits, long long u, float m) {
+  long long lo = 0, len = n;
+  for (int b = bits - 1; b >= 0; --b) {
+    const long long c = (len + 1) >> 1;
+    if ((u >> b) & 1) { lo += c; len -= c; } else { len = c; }
+  }
+  if (len <= kPwLeaf) return pw_leaf<SQ>(x + lo, len, m);
+  const long long c = (len + 1) >> 1;
+  const float a = pw_leaf<SQ>(x + lo, c, m);
+  const float b = pw_leaf<SQ>(x + lo + c, len - c, m);
+  return __fadd_rn(a, b);
+}
+
+// Pairwise (perfect binary tree, left + right) combination of S values, S a power of two.
+__device__ __forceinline__ float pw_tree(const float* __restrict__ v, int S) {
+  float stk[32];
+  for (int k = 0; k < S; ++k) {
+    float a = v[k];
+    int lev = 0;
+    while ((k >> lev) & 1) { a = __fadd_rn(stk[lev], a); ++lev; }
+    stk[lev] = a;
+  }
+  int top = 0;
+  while ((1 << top) < S) ++top;
+  return stk[top];
+}
+
+// grid (S, ncols), block T (a power of two <= kPwThreads): CTA (s, col) combines the units
+// [s*T*G, (s+1)*T*G) of column col into part[col*S + s].  With SQ, f(x) = abs2(x - mean of
+// the column), the mean taken from the first pass's partials part_sum.
+template <bool SQ>
+__global__ void __launch_bounds__(kPwThreads)
+pw_units_kernel(const float* const* __restrict__ mats, const float* __restrict__ base, long long Nf,
+                long long Nrb, int bits, long long G, int S, const float* __restrict__ part_sum,
+                float* __restrict__ part) {
+  const long long col = blockIdx.y;
+  const float* x = pw_column(mats, base, Nf, Nrb, col);
+  __shared__ float red[kPwThreads];
+  __shared__ float s_mean;
+  float m = 0.f;
+  if (SQ) {
+    if (threadIdx.x == 0) s_mean = __fdiv_rn(pw_tree(part_sum + col * S, S), (float)Nf);
+    __syncthreads();
+    m = s_mean;
+  }
+  const long long u0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * G;
+  float stk[40];
+  for (long long k = 0; k < G; ++k) {
+    float a = pw_unit<SQ>(x, Nf, bits, u0 + k, m);
+    int lev = 0;
+    while ((k >> lev) & 1) { a = __fadd_rn(stk[lev], a); ++lev; }
+    stk[lev] = a;
+  }
+  int top = 0;
+  while ((1LL << top) < G) ++top;
+  red[threadIdx.x] = stk[top];
+  __syncthreads();
+  for (int w = blockDim.x >> 1; w >= 1; w >>= 1) {
+    float a = 0.f;
+    if ((int)threadIdx.x < w) a = __fadd_rn(red[2 * threadIdx.x], red[2 * threadIdx.x + 1]);
+    __syncthreads();
+    if ((int)threadIdx.x < w) red[threadIdx.x] = a;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[col * S + blockIdx.x] = red[0];
+}
+
+// m = mean of column 0, s = minimum std over the columns (NaN if any is NaN); ms[2] = the
+// fdrdenormalize threshold snr*s + m in Float64 (FDR_SNR_F64) or Float32 (FDR_SNR_F32).
+__global__ void pw_finalize_kernel(const float* __restrict__ part_sum, const float* __restrict__ part_sq,
+                                   long long ncols, int S, long long Nf, int snr_mode, double snr,
+                                   double* __restrict__ ms) {
+  __shared__ float smin[256];
+  __shared__ int snan[256];
+  const float inv = __fdiv_rn(1.0f, (float)(Nf - 1));  // Float32(1 // (n-1))
+  float best = INFINITY;
+  int nan = 0;
+  for (long long c = threadIdx.x; c < ncols; c += blockDim.x) {
+    const float sd = __fsqrt_rn(__fmul_rn(pw_tree(part_sq + c * S, S), inv));
+    if (isnan(sd)) nan = 1; else best = fminf(best, sd);
+  }
+  smin[threadIdx.x] = best;
+  snan[threadIdx.x] = nan;
   __syncthreads();
   if (threadIdx.x == 0) {
-    double a = 0.0, c = 0.0;
-    for (int i = 0; i < kRedThreads / 32; ++i) { a += r1[i]; c += r2[i]; }
-    atomicAdd(acc + 2 * col, a);
-    atomicAdd(acc + 2 * col + 1, c);
+    float b = INFINITY;
+    int anynan = 0;
+    for (int i = 0; i < (int)blockDim.x; ++i) { b = fminf(b, smin[i]); anynan |= snan[i]; }
+    const float m = __fdiv_rn(pw_tree(part_sum, S), (float)Nf);
+    const float s = anynan ? __int_as_float(0x7fc00000) : b;
+    ms[0] = (double)m;
+    ms[1] = (double)s;
+    if (snr_mode == FDR_SNR_F32)
+      ms[2] = (double)__fadd_rn(__fmul_rn((float)snr, s), m);
+    else
+      ms[2] = snr * (double)s + (double)m;
   }
+}
+
+struct PwShape {
+  int bits;     // depth of the units
+  long long M;  // units per column
+  int T;        // threads per CTA
+  int S;        // CTAs (partials) per column
+  long long G;  // units per thread
+};
+
+static PwShape pw_shape(long long n, long long ncols, int smax) {
+  int D = 0;
+  while (cdiv(n, 1LL << D) > kPwLeaf) ++D;
+  PwShape p;
+  p.bits = D > 0 ? D - 1 : 0;
+  p.M = 1LL << p.bits;
+  p.T = (int)std::min<long long>(kPwThreads, p.M);
+  long long S = 1;
+  const long long target = 4LL * sm_count();
+  while (2 * S <= smax && 2 * S * p.T <= p.M && ncols * S < target) S *= 2;
+  p.S = (int)S;
+  p.G = p.M / (S * p.T);
+  return p;
+}
+
+int pairwise_stats_parts(long long Nf, long long ncols, int smax) { return pw_shape(Nf, ncols, smax).S; }
+
+int pairwise_stats_launch(const float* const* d_mats, const float* base, long long nb, long long Nf,
+                          long long Nrb, float* part, int smax, double* d_ms, int snr_mode,
+                          double snr, cudaStream_t s) {
+  const long long ncols = nb * Nrb;
+  FDR_CHECK_ARG(ncols <= 65535, "fdrstats: at most 65535 columns in total");
+  FDR_CHECK_ARG(smax >= 1 && smax <= (1 << 20), "fdrstats: bad partial count");
+  const PwShape p = pw_shape(Nf, ncols, smax);
+  float* part_sum = part;
+  float* part_sq = part + ncols * p.S;
+  const dim3 grid((unsigned)p.S, (unsigned)ncols);
+  pw_units_kernel<false><<<grid, p.T, 0, s>>>(d_mats, base, Nf, Nrb, p.bits, p.G, p.S, nullptr, part_sum);
+  FDR_LAUNCH_CHECK("pw_units_kernel<sum>");
+  pw_units_kernel<true><<<grid, p.T, 0, s>>>(d_mats, base, Nf, Nrb, p.bits, p.G, p.S, part_sum, part_sq);
+  FDR_LAUNCH_CHECK("pw_units_kernel<abs2>");
+  pw_finalize_kernel<<<1, 256, 0, s>>>(part_sum, part_sq, ncols, p.S, Nf, snr_mode, snr, d_ms);
+  FDR_LAUNCH_CHECK("pw_finalize_kernel");
+  return FDR_OK;
 }
 
 // m = mean(column 0); s = min over columns of sqrt(corrected variance).
@@ -168,9 +364,14 @@ protohits_write_kernel(const float* const* __restrict__ mats, long long Nf, long
   }
 }
 
-// thr = snr * Float32(s) + Float32(m)   (fdrdenormalize with the reference's Float32 m, s)
-__global__ void threshold_kernel(const double* __restrict__ ms, double snr, double* __restrict__ thr) {
-  thr[0] = snr * (double)(float)ms[1] + (double)(float)ms[0];
+// fdrdenormalize (fdrutils.jl:104-107) from float64 moments: thr = snr*s + m with m and s
+// rounded to Float32 (the reference's types), in Float64 (FDR_SNR_F64) or Float32
+// (FDR_SNR_F32) arithmetic.
+__global__ void threshold_kernel(const double* __restrict__ ms, int snr_mode, double snr,
+                                 double* __restrict__ thr) {
+  const float m = (float)ms[0], s = (float)ms[1];
+  thr[0] = snr_mode == FDR_SNR_F32 ? (double)__fadd_rn(__fmul_rn((float)snr, s), m)
+                                   : snr * (double)s + (double)m;
 }
 
 // Exclusive scan of counts (single CTA); offsets[n] = total.
@@ -206,23 +407,19 @@ int upload_ptrs(const void* const* host, int64_t nb, void*** dev, cudaStream_t s
   return FDR_OK;
 }
 
-// Stats into a device array ms[2] (no host synchronisation).
-int stats_device(const float* const* d_mats, int64_t nb, int64_t Nf, int64_t Nrb,
-                        double* d_ms, cudaStream_t s) {
+// fdrstats in Float32 pairwise order into the device array ms[3] = (m, s, threshold) (no host
+// synchronisation); the threshold is fdrdenormalize(snr, m, s) for snr_mode FDR_SNR_F64 /
+// FDR_SNR_F32 (unused otherwise).
+int stats_device(const float* const* d_mats, int64_t nb, int64_t Nf, int64_t Nrb, double* d_ms,
+                 int snr_mode, double snr, cudaStream_t s) {
   const long long ncols = nb * Nrb;
-  double* acc = nullptr;
-  FDR_TRY(scratch_alloc((void**)&acc, sizeof(double) * 2 * ncols, s));
-  FDR_CUDA(cudaMemsetAsync(acc, 0, sizeof(double) * 2 * ncols, s));
-  const long long rows_blocks = std::max<long long>(1, std::min<long long>(cdiv(Nf, kRedThreads * 8),
-      std::max<long long>(1, (long long)sm_count() * 8 / std::max<long long>(1, ncols))));
-  FDR_CHECK_ARG(ncols <= 65535, "fdrstats: at most 65535 columns in total");
-  column_moments_kernel<<<dim3((unsigned)rows_blocks, (unsigned)ncols), kRedThreads, 0, s>>>(
-      d_mats, Nf, Nrb, acc);
-  FDR_LAUNCH_CHECK("column_moments_kernel");
-  stats_finalize_kernel<<<1, 256, 0, s>>>(acc, ncols, Nf, d_ms);
-  FDR_LAUNCH_CHECK("stats_finalize_kernel");
-  scratch_free(acc, s);
-  return FDR_OK;
+  const int smax = 256;
+  const int S = pairwise_stats_parts(Nf, ncols, smax);
+  float* part = nullptr;
+  FDR_TRY(scratch_alloc((void**)&part, sizeof(float) * 2 * ncols * S, s));
+  const int st = pairwise_stats_launch(d_mats, nullptr, nb, Nf, Nrb, part, smax, d_ms, snr_mode, snr, s);
+  scratch_free(part, s);
+  return st;
 }
 
 // Per-column float64 sum and sum of squares of one Nf x ncols matrix, added into acc.
@@ -269,8 +466,8 @@ int stats_finalize_launch(const double* acc, long long ncols, long long Nf, doub
   return FDR_OK;
 }
 
-int threshold_launch(const double* d_ms, double snr, double* d_thr, cudaStream_t s) {
-  threshold_kernel<<<1, 1, 0, s>>>(d_ms, snr, d_thr);
+int threshold_launch(const double* d_ms, int snr_mode, double snr, double* d_thr, cudaStream_t s) {
+  threshold_kernel<<<1, 1, 0, s>>>(d_ms, snr_mode, snr, d_thr);
   FDR_LAUNCH_CHECK("threshold_kernel");
   return FDR_OK;
 }
@@ -333,8 +530,8 @@ int fdr_stats(const float* const* fdrs, int64_t nb, int64_t Nf, int64_t Nrb, dou
   void** d_mats = nullptr;
   double* d_ms = nullptr;
   FDR_TRY(upload_ptrs((const void* const*)fdrs, nb, &d_mats, s));
-  FDR_TRY(scratch_alloc((void**)&d_ms, 2 * sizeof(double), s));
-  int st = stats_device((const float* const*)d_mats, nb, Nf, Nrb, d_ms, s);
+  FDR_TRY(scratch_alloc((void**)&d_ms, 3 * sizeof(double), s));
+  int st = stats_device((const float* const*)d_mats, nb, Nf, Nrb, d_ms, 0, 0.0, s);
   double h[2] = {0, 0};
   if (st == FDR_OK) {
     cudaError_t e = cudaMemcpyAsync(h, d_ms, sizeof(h), cudaMemcpyDeviceToHost, s);
@@ -367,6 +564,8 @@ int fdr_findprotohits(const float* const* fdrs, int64_t nb, int64_t Nf, int64_t 
   FDR_CHECK_ARG(fdrs && count, "findprotohits: NULL argument");
   FDR_CHECK_ARG(nb >= 1 && Nf >= 1 && Nrb >= 1, "findprotohits: bad sizes");
   FDR_CHECK_ARG(capacity >= 0 && (capacity == 0 || hits != nullptr), "findprotohits: bad hit buffer");
+  FDR_CHECK_ARG(snr == 0 || snr == FDR_SNR_F64 || snr == FDR_SNR_F32,
+                "findprotohits: snr must be 0, FDR_SNR_F64 or FDR_SNR_F32 (got %d)", snr);
   for (int64_t b = 0; b < nb; ++b) FDR_CHECK_ARG(fdrs[b] != nullptr, "findprotohits: matrix %lld is NULL", (long long)b);
   cudaStream_t s = (cudaStream_t)stream;
   *count = 0;
@@ -377,8 +576,7 @@ int fdr_findprotohits(const float* const* fdrs, int64_t nb, int64_t Nf, int64_t 
   if (snr) {
     st = scratch_alloc((void**)&d_ms, 3 * sizeof(double), s);
     // fdrdenormalize(snr, fdrs) = snr*s + m with the reference's Float32 m and s
-    if (st == FDR_OK) st = stats_device((const float* const*)d_mats, nb, Nf, Nrb, d_ms, s);
-    if (st == FDR_OK) st = threshold_launch(d_ms, threshold, d_ms + 2, s);
+    if (st == FDR_OK) st = stats_device((const float* const*)d_mats, nb, Nf, Nrb, d_ms, snr, threshold, s);
   }
   if (st == FDR_OK)
     st = hits_run((const float* const*)d_mats, nb, Nf, Nrb, threshold, snr ? d_ms + 2 : nullptr,

@@ -500,20 +500,30 @@ int fdr_zdtfdr_protohits(fdr_zdt* ws, const float* spectrogram, const float* r0s
   FDR_CHECK_ARG(ws != nullptr && count != nullptr, "zdtfdr_protohits: NULL argument");
   FDR_CHECK_ARG(nbatch >= 1, "zdtfdr_protohits: need at least one dest");
   FDR_CHECK_ARG(capacity >= 0 && (capacity == 0 || hits != nullptr), "zdtfdr_protohits: bad hit buffer");
+  FDR_CHECK_ARG(snr == 0 || snr == FDR_SNR_F64 || snr == FDR_SNR_F32,
+                "zdtfdr_protohits: snr must be 0, FDR_SNR_F64 or FDR_SNR_F32 (got %d)", snr);
   *count = 0;
   cudaStream_t s = (cudaStream_t)stream;
   const int64_t ncols = nbatch * ws->Nr;
-  double* acc = nullptr;  // 2*ncols moments, then m, s, threshold
+  const bool fast = (ws->flags & FDR_ZDT_FAST_STATS) != 0;
+  double* acc = nullptr;  // [2*ncols moments (fast statistics)], then m, s, threshold
   if (snr) {
-    FDR_TRY(scratch_alloc((void**)&acc, sizeof(double) * (2 * ncols + 3), s));
-    FDR_CUDA(cudaMemsetAsync(acc, 0, sizeof(double) * 2 * ncols, s));
+    FDR_TRY(scratch_alloc((void**)&acc, sizeof(double) * ((fast ? 2 * ncols : 0) + 3), s));
+    if (fast) FDR_CUDA(cudaMemsetAsync(acc, 0, sizeof(double) * 2 * ncols, s));
   }
-  int st = zdt_execute(ws, spectrogram, r0s, nbatch, dests, window, custom_window, acc, stream);
-  double* d_ms = acc ? acc + 2 * ncols : nullptr;
-  if (st == FDR_OK && snr) st = stats_finalize_launch(acc, ncols, ws->Nf, d_ms, s);
-  if (st == FDR_OK && snr) st = threshold_launch(d_ms, threshold, d_ms + 2, s);
+  int st = zdt_execute(ws, spectrogram, r0s, nbatch, dests, window, custom_window,
+                       fast ? acc : nullptr, stream);
+  double* d_ms = acc ? acc + (fast ? 2 * ncols : 0) : nullptr;
   void** d_mats = nullptr;
   if (st == FDR_OK) st = upload_ptrs((const void* const*)dests, nbatch, &d_mats, s);
+  if (st == FDR_OK && snr) {
+    if (fast) {
+      st = stats_finalize_launch(acc, ncols, ws->Nf, d_ms, s);
+      if (st == FDR_OK) st = threshold_launch(d_ms, snr, threshold, d_ms + 2, s);
+    } else {
+      st = stats_device((const float* const*)d_mats, nbatch, ws->Nf, ws->Nr, d_ms, snr, threshold, s);
+    }
+  }
   if (st == FDR_OK)
     st = hits_run((const float* const*)d_mats, nbatch, ws->Nf, ws->Nr, threshold,
                   snr ? d_ms + 2 : nullptr, hits, capacity, count, threshold_used, s);
@@ -536,21 +546,31 @@ int fdr_zdtfdr_blocks_protohits(fdr_zdt* ws, const float* spectrogram, const int
   FDR_CHECK_ARG(ws != nullptr && count != nullptr, "zdtfdr_blocks_protohits: NULL argument");
   FDR_CHECK_ARG(nblocks >= 1, "zdtfdr_blocks_protohits: need at least one block");
   FDR_CHECK_ARG(capacity >= 0 && (capacity == 0 || hits != nullptr), "zdtfdr_blocks_protohits: bad hit buffer");
+  FDR_CHECK_ARG(snr == 0 || snr == FDR_SNR_F64 || snr == FDR_SNR_F32,
+                "zdtfdr_blocks_protohits: snr must be 0, FDR_SNR_F64 or FDR_SNR_F32 (got %d)", snr);
   *count = 0;
   cudaStream_t s = (cudaStream_t)stream;
   const int64_t ncols = 8 * nblocks;
-  double* acc = nullptr;  // 2*ncols moments, then m, s, threshold
+  const bool fast = (ws->flags & FDR_ZDT_FAST_STATS) != 0;
+  double* acc = nullptr;  // [2*ncols moments (fast statistics)], then m, s, threshold
   if (snr) {
-    FDR_TRY(scratch_alloc((void**)&acc, sizeof(double) * (2 * ncols + 3), s));
-    FDR_CUDA(cudaMemsetAsync(acc, 0, sizeof(double) * 2 * ncols, s));
+    FDR_TRY(scratch_alloc((void**)&acc, sizeof(double) * ((fast ? 2 * ncols : 0) + 3), s));
+    if (fast) FDR_CUDA(cudaMemsetAsync(acc, 0, sizeof(double) * 2 * ncols, s));
   }
-  int st = zdt_execute_blocks(ws, spectrogram, blocks, nblocks, dest, window, custom_window, acc, s);
-  double* d_ms = acc ? acc + 2 * ncols : nullptr;
-  if (st == FDR_OK && snr) st = stats_finalize_launch(acc, ncols, ws->Nf, d_ms, s);
-  if (st == FDR_OK && snr) st = threshold_launch(d_ms, threshold, d_ms + 2, s);
+  int st = zdt_execute_blocks(ws, spectrogram, blocks, nblocks, dest, window, custom_window,
+                              fast ? acc : nullptr, s);
+  double* d_ms = acc ? acc + (fast ? 2 * ncols : 0) : nullptr;
   void** d_mats = nullptr;
   float* const dl[1] = {dest};
   if (st == FDR_OK) st = upload_ptrs((const void* const*)dl, 1, &d_mats, s);
+  if (st == FDR_OK && snr) {
+    if (fast) {
+      st = stats_finalize_launch(acc, ncols, ws->Nf, d_ms, s);
+      if (st == FDR_OK) st = threshold_launch(d_ms, snr, threshold, d_ms + 2, s);
+    } else {
+      st = stats_device((const float* const*)d_mats, 1, ws->Nf, ncols, d_ms, snr, threshold, s);
+    }
+  }
   if (st == FDR_OK)
     st = hits_run((const float* const*)d_mats, 1, ws->Nf, ncols, threshold,
                   snr ? d_ms + 2 : nullptr, hits, capacity, count, threshold_used, s);

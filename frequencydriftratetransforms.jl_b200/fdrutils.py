@@ -27,8 +27,8 @@ def create_fdr(spectrogram, Nr_or_rates):
 
 
 def fdrstats(fdr, stream=None):
-    """fdrstats (fdrutils.jl:39-50) -> (m, s) as float32 values (the reference's types);
-    accumulated in float64 on the device."""
+    """fdrstats (fdrutils.jl:39-50) -> (m, s) as float32 values, computed on the device in
+    Float32 in the order of the reference's pairwise sums (fdr_stats)."""
     mats, _ = _mats(fdr)
     Nf, Nrb = mats[0].shape
     m, s = C.c_double(), C.c_double()
@@ -55,12 +55,17 @@ def fdrnormalize_(fdr, m=None, s=None, stream=None):
 
 
 def fdrdenormalize(snr, m_or_fdr, s=None, stream=None):
-    """fdrdenormalize (fdrutils.jl:104-119)."""
+    """fdrdenormalize (fdrutils.jl:104-119): snr*s + m in Julia's promoted type -- Float32
+    for an integer or numpy float32 snr with Float32 m and s (each operation rounded),
+    Float64 for a Python float snr."""
     if s is None:
         m, s = fdrstats(m_or_fdr, stream)
     else:
         m = m_or_fdr
-    return snr * float(s) + float(m)
+    if (isinstance(snr, (bool, int, np.integer, np.float32)) and isinstance(m, np.float32)
+            and isinstance(s, np.float32)):
+        return np.float32(np.float32(np.float32(snr) * s) + m)
+    return float(snr) * float(s) + float(m)
 
 
 def fdrsynchronize(_type=None):
@@ -70,7 +75,10 @@ def fdrsynchronize(_type=None):
 
 def findprotohits(fdr, threshold, snr=False, capacity=None, stream=None, return_threshold=False):
     """findprotohits (fdrutils.jl:148-169) -> int64 numpy array (nhits, 2) of ZERO-based
-    (i, j) in column-major order (j offset by b*Nrb for the b-th matrix of a list)."""
+    (i, j) in column-major order (j offset by b*Nrb for the b-th matrix of a list).  With
+    ``snr`` the threshold is fdrdenormalize(threshold, fdr) in the type Julia promotes
+    ``threshold`` to: an int (or numpy float32) threshold gives Float32 arithmetic and
+    comparison, a float gives Float64."""
     mats, _ = _mats(fdr)
     Nf, Nrb = mats[0].shape
     for mm in mats:
@@ -83,7 +91,7 @@ def findprotohits(fdr, threshold, snr=False, capacity=None, stream=None, return_
         count = C.c_int64()
         thr = C.c_double()
         st = _lib.lib().fdr_findprotohits(_ptr_array(mats), len(mats), Nf, Nrb,
-                                          float(threshold), 1 if snr else 0, ptr(hits),
+                                          float(threshold), _lib.snr_mode(threshold, snr), ptr(hits),
                                           capacity, C.byref(count), C.byref(thr),
                                           stream_handle(stream))
         if st == _lib.FDR_ERR_CAPACITY:

@@ -46,12 +46,15 @@ class ZDTWorkspace:
     ``staged_only`` (zdtfdr_ always runs the staged kernels) and ``mixed_precision`` (the
     fused output pass runs its DFTs as split-bfloat16 tensor-core contractions where the
     four-step split has P = 1024: Nf = 2^19 and, since such a workspace splits Nf = 2^20 as
-    1024 x 1024, Nf = 2^20 with Nt <= 16; ~1e-5 relative error instead of ~1e-6).
+    1024 x 1024, Nf = 2^20 with Nt <= 16; ~1e-5 relative error instead of ~1e-6) and
+    ``fast_stats`` (the snr statistics of ``zdtfdr_protohits_`` come from float64 moments
+    accumulated while the FDR is written: two fewer FDR reads, last bits of m and s may
+    differ from the reference's Float32 values).
     """
 
     def __init__(self, spectrogram, r0_or_rates, dr=None, Nr=None, factors=(2, 3, 5), *,
                  output_aligned=False, exact_phase=False, staged_only=False, mixed_precision=False,
-                 shape=None, stream=None):
+                 fast_stats=False, shape=None, stream=None):
         if dr is None:
             r0, dr, Nr = _range_params(r0_or_rates)
         else:
@@ -71,6 +74,8 @@ class ZDTWorkspace:
             flags |= _lib.FDR_ZDT_STAGED_ONLY
         if mixed_precision:
             flags |= _lib.FDR_ZDT_MIXED_PRECISION
+        if fast_stats:
+            flags |= _lib.FDR_ZDT_FAST_STATS
         farr, nf = _lib.i64_array([int(f) for f in factors])
         h = C.c_void_p()
         _lib.check(_lib.lib().fdr_zdt_create(
@@ -281,9 +286,12 @@ def zdtfdr_protohits_(dests, ws: ZDTWorkspace, spectrogram=None, *, r0=None, w="
                       threshold=10.0, snr=True, capacity=None, stream=None,
                       return_threshold=False):
     """zdtfdr!(dests, ws[, spectrogram]; r0) followed by findprotohits(dests, threshold; snr)
-    with the fused threshold/proto-hit scan of the library (fdr_zdtfdr_protohits): the
-    statistics are accumulated while the FDR is written.  Returns an int64 numpy array of
-    zero-based (i, j) hits in column-major order (j offset by b*Nr for the b-th dest)."""
+    with the fused threshold/proto-hit scan of the library (fdr_zdtfdr_protohits): with
+    ``snr`` the statistics are fdrstats's Float32 pairwise values over the dests (or, for a
+    workspace made with ``fast_stats=True``, float64 moments accumulated while the FDR is
+    written), and the threshold's type follows ``threshold`` as in findprotohits.  Returns
+    an int64 numpy array of zero-based (i, j) hits in column-major order (j offset by b*Nr
+    for the b-th dest)."""
     single = isinstance(dests, torch.Tensor)
     dl = [dests] if single else list(dests)
     for d in dl:
@@ -307,7 +315,8 @@ def zdtfdr_protohits_(dests, ws: ZDTWorkspace, spectrogram=None, *, r0=None, w="
     hits = torch.empty((max(1, cap), 2), dtype=torch.int64, device="cuda")
     count, thr = C.c_int64(), C.c_double()
     st = _lib.lib().fdr_zdtfdr_protohits(ws._h, ptr(spec), r0_arr, n, d_arr, code, ptr(vals),
-                                         float(threshold), 1 if snr else 0, ptr(hits), cap,
+                                         float(threshold), _lib.snr_mode(threshold, snr),
+                                         ptr(hits), cap,
                                          C.byref(count), C.byref(thr), stream_handle(stream))
     if vals is not None:
         torch.cuda.current_stream().synchronize()
@@ -365,7 +374,8 @@ def zdtfdr_blocks_protohits_(dest, ws: ZDTWorkspace, spectrogram, blocks, *, w="
     hits = torch.empty((max(1, cap), 2), dtype=torch.int64, device="cuda")
     count, thr = C.c_int64(), C.c_double()
     st = _lib.lib().fdr_zdtfdr_blocks_protohits(ws._h, ptr(spec), barr, nb, ptr(dest), code,
-                                                ptr(vals), float(threshold), 1 if snr else 0,
+                                                ptr(vals), float(threshold),
+                                                _lib.snr_mode(threshold, snr),
                                                 ptr(hits), cap, C.byref(count), C.byref(thr),
                                                 stream_handle(stream))
     if vals is not None:

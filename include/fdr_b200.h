@@ -65,6 +65,22 @@ typedef enum fdr_window {
                                        ~1e-5 of the FDR's peak instead of ~1e-6; no
                                        counterpart in the reference) */
 
+#define FDR_ZDT_FAST_STATS 0x10u     /* the snr statistics of the fused proto-hit scan
+                                       (fdr_zdtfdr_protohits) come from float64 column moments
+                                       accumulated while the FDR is written: two fewer reads
+                                       of the FDR, but m and s may differ from the reference's
+                                       Float32 pairwise values in the last bits (default: the
+                                       Float32 pairwise values of fdr_stats) */
+
+/* `snr` argument of the proto-hit searches: 0 = `threshold` is the threshold itself;
+   otherwise findprotohits(...; snr=true) computes fdrdenormalize(threshold, fdrs) =
+   threshold*s + m (fdrutils.jl:104-107) in Julia's promoted type of `threshold`:
+   FDR_SNR_F64 for a Float64 snr (Float64 arithmetic and comparison), FDR_SNR_F32 for an
+   Int or Float32 snr (Float32 arithmetic: Float32(snr)*s rounded, + m rounded; Float32
+   comparison). */
+#define FDR_SNR_F64 1
+#define FDR_SNR_F32 2
+
 /* Rate arithmetic for intshift/intfdr (round(rate*(t-1)) in the rate's element type). */
 #define FDR_RATES_F64 0
 #define FDR_RATES_F32 1
@@ -156,10 +172,12 @@ int fdr_zdt_execute(fdr_zdt* ws, const float* spectrogram, const float* r0s, int
                     fdr_stream_t stream);
 /* The fused threshold/proto-hit scan: zdtfdr!(dests, ws[, spectrogram]; r0) followed by
    findprotohits(dests, threshold; snr) (zdtfdr.jl:349-378, fdrutils.jl:148-169).  With snr,
-   the column statistics of fdrstats (fdrutils.jl:39-50) are accumulated while the FDR
-   columns are written, so the FDR is read once more only to count the proto-hits (tiles
-   without hits are not re-read by the write pass).  Hits, count and threshold as in
-   fdr_findprotohits (the batches are the hcat'd matrices).  Synchronises `stream`. */
+   the statistics are fdr_stats's Float32 pairwise values over the dests (two reads of the
+   FDR), or, for a workspace created with FDR_ZDT_FAST_STATS, float64 column moments
+   accumulated while the FDR columns are written (no extra read).  The FDR is then read
+   once more to count the proto-hits (tiles without hits are not re-read by the write
+   pass).  Hits, count and threshold as in fdr_findprotohits (the batches are the hcat'd
+   matrices).  Synchronises `stream`. */
 int fdr_zdtfdr_protohits(fdr_zdt* ws, const float* spectrogram, const float* r0s, int64_t nbatch,
                          float* const* dests, int window, const double* custom_window,
                          double threshold, int snr, int64_t* hits, int64_t capacity,
@@ -317,23 +335,31 @@ int fdr_fftfdr(fdr_fft_ws* ws, const float* rates, int64_t Nr, float* fdr,
 /* ---------------------------------------------------------------------------------- */
 /* fdrstats (fdrutils.jl:39-50) over nb matrices (HOST array of nb device pointers), each
    Nf x Nrb with leading dimension Nf: m = mean of column 1 of the first matrix,
-   s = minimum over all columns of the corrected standard deviation.  Accumulates in
-   float64.  Synchronises `stream` and writes host doubles. */
+   s = minimum over all columns of the corrected standard deviation (NaN if any is NaN).
+   Computed in Float32 in the order of Julia's CPU code: each column is reduced by Base's
+   pairwise mapreduce (blocks of at most 1024 elements summed sequentially, combined
+   pairwise), mean = sum / Float32(Nf), variance = pairwise sum of abs2(x - mean) times
+   Float32(1 // (Nf - 1)) (Statistics.varm!), std = sqrt.  Deterministic.  Julia's @simd
+   block loop may reassociate on its host, so the reference's own last bits of m and s can
+   differ from these on some CPUs.  Synchronises `stream` and writes the Float32 values as
+   host doubles. */
 int fdr_stats(const float* const* fdrs, int64_t nb, int64_t Nf, int64_t Nrb, double* m,
               double* s, fdr_stream_t stream);
 /* fdrstats of a single FDR matrix without allocating device memory.  This entry point has
    no counterpart in the reference; it serves callers that must not allocate once they are
    running -- e.g. a real-time pipeline (an allocation can stall on the device or fail when
    memory is short) or a host whose device memory is entirely held by its own pool
-   allocator.  Same results as fdr_stats for nb = 1 (float64 accumulation; the summation
-   order may differ in the last bits).  Its scratch space is a fixed file-scope device array
-   sized for at most FDR_STATS_NOALLOC_MAX_COLUMNS columns (16 bytes per column plus 16),
-   which every GPU that loads the library keeps until the process exits; larger Nr is
-   rejected with FDR_ERR_INVALID_ARGUMENT.  All calls share that array: calls whose work
-   overlaps on the GPU (different streams or devices' threads racing on one device) race,
-   so serialise them.  The first call on a device looks up the array's device address
+   allocator.  Same results as fdr_stats for nb = 1, bit for bit (the same Float32 pairwise
+   kernels).  Its scratch space is a fixed file-scope device array sized for at most
+   FDR_STATS_NOALLOC_MAX_COLUMNS columns (16 bytes per column plus 32), which every GPU that
+   loads the library keeps until the process exits; larger Nr is rejected with
+   FDR_ERR_INVALID_ARGUMENT.  Every call writes all the scratch it reads, so no state carries
+   over from the previous call.  All calls share that array: any two calls on one device
+   whose work may interleave race -- calls on different streams, and calls that two host
+   threads enqueue on the same stream -- so serialise the calls on the host.  The first call
+   on a device (and CUDA context) looks up the array's device address
    (cudaGetSymbolAddress) with that device current; make that first call before any stream
-   capture.  Synchronises `stream` and writes host doubles. */
+   capture begins.  Synchronises `stream` and writes host doubles. */
 #define FDR_STATS_NOALLOC_MAX_COLUMNS 8192
 int fdr_stats_noalloc(const float* fdr, int64_t Nf, int64_t Nr, double* m, double* s,
                       fdr_stream_t stream);
@@ -344,9 +370,10 @@ int fdr_normalize(float* const* fdrs, int64_t nb, int64_t Nf, int64_t Nrb, float
    with fdr[i, j] >= threshold, in column-major (findall) order, written as ZERO-based
    int64 pairs hits[2*h] = i, hits[2*h+1] = j (device buffer of 2*capacity int64).
    Each float32 element is compared with the float64 threshold (Julia promotes the
-   Float32 element for `>=(threshold)` with a Float64 threshold).  snr != 0 replaces
-   `threshold` by fdrdenormalize(threshold, fdrs) = threshold*s + m, formed in float64
-   from the float32-rounded m and s.  Synchronises `stream`; *count (host) receives the
+   Float32 element for `>=(threshold)` with a Float64 threshold).  snr = FDR_SNR_F64 or
+   FDR_SNR_F32 replaces `threshold` by fdrdenormalize(threshold, fdrs) = threshold*s + m
+   with fdr_stats's m and s, in Float64 or Float32 arithmetic as Julia promotes a Float64
+   or an Int/Float32 snr.  Synchronises `stream`; *count (host) receives the
    total number of hits; if it exceeds `capacity`, the first `capacity` hits are written
    and FDR_ERR_CAPACITY is returned.  *threshold_used (host, may be NULL) receives the
    threshold compared against. */

@@ -474,9 +474,96 @@ def zdtfdr(spec, r0, dr, Nr, factors=(2, 3, 5), window="rect", workers=None):
 # fdrutils.jl
 # ----------------------------------------------------------------------------------------
 
+PAIRWISE_BLOCKSIZE = 1024  # Base.pairwise_blocksize(f, op) for sum-like reductions
+
+
+def pairwise_leaves(n, blk=PAIRWISE_BLOCKSIZE):
+    """Leaves of Base.mapreduce_impl(f, op, A, 1, n, blk) (Julia base/reduce.jl): a range
+    [lo, hi] (1-based, inclusive) with lo == hi or hi - lo < blk is summed sequentially;
+    any other range splits at mid = lo + (hi - lo) >> 1 into [lo, mid] and [mid+1, hi].
+    Returned as zero-based half-open (start, stop) pairs, left to right."""
+    out = []
+    stack = [(1, int(n))]
+    while stack:
+        lo, hi = stack.pop()
+        if lo == hi or hi - lo < blk:
+            out.append((lo - 1, hi))
+        else:
+            mid = lo + ((hi - lo) >> 1)
+            stack.append((mid + 1, hi))
+            stack.append((lo, mid))
+    return out
+
+
+def pairwise_sum32(cols, f=None, blk=PAIRWISE_BLOCKSIZE):
+    """Float32 sum of every column of ``cols`` (n, ncols) in the order of Julia's pairwise
+    mapreduce: each leaf of ``pairwise_leaves(n)`` is summed sequentially,
+    ((f(a1) + f(a2)) + f(a3)) + ..., and the leaves are combined as op(v_left, v_right) up
+    the recursion.  ``f`` (float32 -> float32, elementwise on numpy arrays) defaults to
+    the identity.
+
+    The sequential leaf loop of mapreduce_impl carries Julia's ``@simd`` annotation, which
+    lets LLVM reassociate it into vector lanes whose width depends on the host CPU; this
+    restatement takes the loop's written (sequential) order."""
+    x = np.asarray(cols, dtype=np.float32)
+    if x.ndim == 1:
+        x = x[:, None]
+    n = x.shape[0]
+    fx = x if f is None else np.asarray(f(x), dtype=np.float32)
+    leaves = pairwise_leaves(n, blk)
+    # sequential sums of all leaves at once: leaf l, step i adds fx[start_l + i]
+    starts = np.array([a for a, _ in leaves], dtype=np.int64)
+    lens = np.array([b - a for a, b in leaves], dtype=np.int64)
+    acc = fx[starts].copy()                                   # (nleaves, ncols)
+    for i in range(1, int(lens.max())):
+        live = lens > i
+        idx = starts[live] + i
+        acc[live] = (acc[live] + fx[idx]).astype(np.float32)
+    vals = iter(list(acc))
+
+    def rec(lo, hi):  # same recursion as pairwise_leaves, leaves consumed left to right
+        if lo == hi or hi - lo < blk:
+            return next(vals)
+        mid = lo + ((hi - lo) >> 1)
+        a = rec(lo, mid)
+        b = rec(mid + 1, hi)
+        return (a + b).astype(np.float32)
+
+    return rec(1, n)
+
+
+def _std32_columns(M):
+    """std(M, dims=1) in Float32 as Statistics.jl computes it (corrected): column means
+    mean(M, dims=1) = pairwise sum ./ n; varm! = centralize_sumabs2! (pairwise sum of
+    abs2(x - mean)) .* Float32(1 // (n-1)); then sqrt."""
+    M = np.asarray(M, dtype=np.float32)
+    n = M.shape[0]
+    means = (pairwise_sum32(M) / np.float32(n)).astype(np.float32)
+    ss = pairwise_sum32(M, f=lambda v: np.square((v - means).astype(np.float32)))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        inv = np.float32(1.0) / np.float32(n - 1)
+        var = (ss * inv).astype(np.float32)
+        return np.sqrt(var).astype(np.float32)
+
+
 def fdrstats(fdr):
-    """src/fdrutils.jl:39-50, computed in float64 (m = mean of column 1, s = minimum over
-    columns of the corrected standard deviation).  ``fdr`` may be a list of matrices."""
+    """src/fdrutils.jl:39-50 in the reference's Float32 arithmetic: m = mean(fdr[:,1])
+    (Statistics.mean: the pairwise Float32 sum of Base.mapreduce_impl divided by
+    Float32(n)) of the first matrix; s = minimum over all columns (of all matrices) of
+    std(fdr, dims=1) (see ``_std32_columns``), NaN if any column's std is NaN.  Returns
+    (m, s) as numpy float32.  ``fdr`` may be a list of matrices."""
+    mats = fdr if isinstance(fdr, (list, tuple)) else [fdr]
+    c0 = np.asarray(mats[0], dtype=np.float32)[:, :1]
+    m = np.float32((pairwise_sum32(c0) / np.float32(c0.shape[0]))[0])
+    stds = np.concatenate([_std32_columns(M) for M in mats])
+    s = np.float32(np.nan) if np.isnan(stds).any() else np.float32(stds.min())
+    return m, s
+
+
+def fdrstats_f64(fdr):
+    """fdrstats (src/fdrutils.jl:39-50) accumulated in float64 (the statistics of the
+    library's fused-moment option, which differ from the reference's Float32 pairwise
+    values in the last bits)."""
     mats = fdr if isinstance(fdr, (list, tuple)) else [fdr]
     m = float(np.mean(np.asarray(mats[0][:, 0], dtype=np.float64)))
     s = min(float(np.min(np.std(np.asarray(M, dtype=np.float64), axis=0, ddof=1)))
@@ -490,23 +577,32 @@ def fdrnormalize(fdr, m, s):
 
 
 def fdrdenormalize(snr, m, s):
-    """src/fdrutils.jl:104-107."""
-    return snr * s + m
+    """src/fdrutils.jl:104-107: snr * s + m in Julia's promoted type.  m and s are the
+    Float32 values of fdrstats.  An integer or numpy float32 ``snr`` gives Float32
+    arithmetic (Int * Float32 -> Float32, each operation rounded, no fused multiply-add);
+    a Python/numpy float64 ``snr`` gives Float64 arithmetic."""
+    m32, s32 = np.float32(m), np.float32(s)
+    if isinstance(snr, (int, np.integer, np.float32)):
+        return np.float32(np.float32(np.float32(snr) * s32) + m32)
+    return float(snr) * float(s32) + float(m32)
 
 
 def findprotohits(fdr, threshold, snr=False):
     """src/fdrutils.jl:148-169.  Returns an (nhits, 2) int64 array of ZERO-based (i, j)
-    in column-major (findall) order; for a list of matrices, j is offset by b*Nrb."""
+    in column-major (findall) order; for a list of matrices, j is offset by b*Nrb.  Each
+    Float32 element is compared with the threshold exactly (Julia compares mixed Float32 /
+    Float64 / Int values exactly).  With ``snr`` the threshold is fdrdenormalize(threshold,
+    fdrstats(fdr)) in the promoted type of ``threshold`` (see ``fdrdenormalize``)."""
     mats = fdr if isinstance(fdr, (list, tuple)) else [fdr]
     thr = threshold
     if snr:
         m, s = fdrstats(mats)
         thr = fdrdenormalize(threshold, m, s)
-    thr32 = np.float32(thr)
+    thr64 = float(thr)
     out = []
     Nrb = mats[0].shape[1]
     for b, M in enumerate(mats):
-        j, i = np.nonzero(np.asarray(M, dtype=np.float32).T >= thr32)
+        j, i = np.nonzero(np.asarray(M, dtype=np.float32).T.astype(np.float64) >= thr64)
         out.append(np.stack([i, j + b * Nrb], axis=1))
     if not out:
         return np.zeros((0, 2), dtype=np.int64)
@@ -742,3 +838,63 @@ def taylor_tree(spec, dmin, dmax):
             if (d >= 0) == (sgn > 0):
                 out[:, d - dmin] = A[abs(d)]
     return out
+
+
+# ----------------------------------------------------------------------------------------
+# Threaded CPU restatement of zdtfdr! for timing the reference's CPU path
+# ----------------------------------------------------------------------------------------
+
+class ThreadedZDT:
+    """zdtfdr!(dest, ws, spectrogram) restated for speed on the host cores, for timing the
+    reference's CPU path (the reference itself is Julia + FFTW, which is not installed).
+    Same stage order as src/zdtfdr.jl:349-362 -- input! (rfft), preprocess! (prephase
+    multiply and zero fill of Y), convolve! (FFT over l, x V, normalised inverse FFT),
+    postprocess! (postphase multiply), output! (normalised irfft) -- with the chirp factors
+    computed per call from the reference's Float32 phase arguments (prephase_arg,
+    postphase_arg), as the reference's broadcasts do.  Arithmetic is complex64 (numpy's
+    complex multiply, not the per-component rounding of ``_cmul32``); FFTs are scipy
+    pocketfft with ``workers`` threads; the elementwise stages run on row blocks in a pool
+    of ``workers`` threads.  V is built once, as ZDTWorkspace does."""
+
+    def __init__(self, spec, r0, dr, Nr, workers=None, factors=(2, 3, 5)):
+        import concurrent.futures as cf
+        import os
+        spec = np.asarray(spec, dtype=np.float32)
+        self.Nf, self.Nt = spec.shape
+        self.r0, self.dr, self.Nr = np.float32(r0), np.float32(dr), int(Nr)
+        self.Nl = calcNl(self.Nt, self.Nr, factors)
+        self.K = self.Nf // 2 + 1
+        self.workers = int(workers or os.cpu_count() or 1)
+        self.pool = cf.ThreadPoolExecutor(self.workers)
+        self.V = ZDTWorkspace(spec, r0, dr, Nr, factors, workers=self.workers).V  # (K, Nl)
+        self.Y = np.empty((self.K, self.Nl), dtype=np.complex64)
+        self.F = None
+        bl = max(1, -(-self.K // (4 * self.workers)))
+        self.blocks = [(a, min(self.K, a + bl)) for a in range(0, self.K, bl)]
+
+    def _par(self, fn):
+        list(self.pool.map(lambda ab: fn(*ab), self.blocks))
+
+    def zdtfdr(self, spec):
+        f = _fft_mod()
+        w = {"workers": self.workers} if _sfft is not None else {}
+        spec = np.asarray(spec, dtype=np.float32)
+        self.F = f.rfft(spec, axis=0, **w).astype(np.complex64, copy=False)     # input!
+        Nt, Nr, Nf = self.Nt, self.Nr, self.Nf
+        lt = np.arange(Nt)[None, :]
+        lr = np.arange(Nr)[None, :]
+
+        def pre(a, b):                                                          # preprocess!
+            k = np.arange(a, b)[:, None]
+            self.Y[a:b, :Nt] = self.F[a:b] * cispi32(prephase_arg(k, lt, self.r0, self.dr, Nf))
+            self.Y[a:b, Nt:] = 0
+        self._par(pre)
+        Y = f.fft(self.Y, axis=1, **w)                                          # convolve!
+        self._par(lambda a, b: np.multiply(Y[a:b], self.V[a:b], out=Y[a:b]))
+        Y = f.ifft(Y, axis=1, overwrite_x=True, **w)
+
+        def post(a, b):                                                         # postprocess!
+            k = np.arange(a, b)[:, None]
+            Y[a:b, :Nr] *= cispi32(postphase_arg(k, lr, self.dr, Nf))
+        self._par(post)
+        return f.irfft(Y[:, :Nr], n=Nf, axis=0, **w).astype(np.float32, copy=False)  # output!

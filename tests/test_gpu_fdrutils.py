@@ -14,14 +14,27 @@ def _fdr(oracle, Nf=65536, Nr=33, seed=1):
 
 
 def test_stats(fdr, oracle):
+    """fdrstats in the reference's Float32 pairwise order: bit-exact with the oracle."""
     a = _fdr(oracle)
     m, s = fdr.fdrstats(fdr.as_device_f32(a))
     mr, sr = oracle.fdrstats(a)
-    assert abs(m - mr) <= 1e-6 * abs(mr) and abs(s - sr) <= 1e-6 * sr
+    assert (m, s) == (mr, sr)
     b = _fdr(oracle, seed=2)
     m2, s2 = fdr.fdrstats([fdr.as_device_f32(a), fdr.as_device_f32(b)])
-    mr2, sr2 = oracle.fdrstats([a, b])
-    assert abs(m2 - mr2) <= 1e-6 * abs(mr2) and abs(s2 - sr2) <= 1e-6 * sr2
+    assert (m2, s2) == oracle.fdrstats([a, b])
+
+
+@pytest.mark.parametrize("Nf,Nr", [(1, 3), (2, 2), (15, 4), (16, 3), (17, 5), (1024, 3), (1025, 2),
+                                   (3000, 7), (8195, 3), (12289, 2), (1 << 16, 1), (100003, 2)])
+def test_stats_ragged_lengths_bit_exact(fdr, oracle, Nf, Nr):
+    """Column lengths whose pairwise recursion has leaves at two depths, single-element
+    columns (std NaN: 0 * Float32(1//0)) and unaligned leaves."""
+    rng = np.random.default_rng(Nf * 7 + Nr)
+    a = (rng.exponential(1.0, (Nf, Nr)) * 16).astype(np.float32)
+    m, s = fdr.fdrstats(fdr.as_device_f32(a))
+    mr, sr = oracle.fdrstats(a)
+    assert m == mr
+    assert (np.isnan(s) and np.isnan(sr)) or s == sr
 
 
 def test_normalize_bit_exact(fdr, oracle):
@@ -46,13 +59,13 @@ def test_findprotohits_exact(fdr, oracle, thr):
 def test_findprotohits_snr_and_batches(fdr, oracle):
     a, b = _fdr(oracle, seed=3), _fdr(oracle, seed=4)
     ga, gb = fdr.as_device_f32(a), fdr.as_device_f32(b)
-    hits, thr = fdr.findprotohits([ga, gb], 8.0, snr=True, return_threshold=True)
     mr, sr = oracle.fdrstats([a, b])
-    thr_ref = 8.0 * float(np.float32(sr)) + float(np.float32(mr))
-    assert abs(thr - thr_ref) <= 1e-6 * thr_ref
-    ref = oracle.findprotohits([a, b], thr)
-    assert np.array_equal(hits, ref)
-    assert hits[:, 1].max() >= a.shape[1]  # offsets of the second matrix
+    for snr in (8.0, 8):  # Float64 and Int snr (Float32 arithmetic)
+        hits, thr = fdr.findprotohits([ga, gb], snr, snr=True, return_threshold=True)
+        thr_ref = oracle.fdrdenormalize(snr, mr, sr)
+        assert thr == float(thr_ref)
+        assert np.array_equal(hits, oracle.findprotohits([a, b], snr, snr=True))
+        assert hits[:, 1].max() >= a.shape[1]  # offsets of the second matrix
 
 
 def test_findprotohits_capacity(fdr, oracle):

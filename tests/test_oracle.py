@@ -190,3 +190,77 @@ def test_taylor_restatement_is_a_path_sum(oracle, fdr):
         assert np.array_equal(out[:, d + Nt - 1], ref.astype(np.float32))
         worst = max(worst, max(abs(p[t] - d * t / (Nt - 1)) for t in range(Nt)))
     assert worst <= 1.0  # within one channel of the straight line (0.67 at Nt = 16)
+
+
+def _julia_pairwise_literal(x, f=lambda v: v, blk=1024):
+    """Element-by-element transliteration of Base.mapreduce_impl (julia base/reduce.jl) in
+    numpy float32 scalars, with the sequential leaf loop in its written order."""
+    def impl(lo, hi):  # 1-based inclusive
+        if lo == hi:
+            return f(x[lo - 1])
+        if hi - lo < blk:
+            v = np.float32(f(x[lo - 1]) + f(x[lo]))
+            for i in range(lo + 2, hi + 1):
+                v = np.float32(v + f(x[i - 1]))
+            return v
+        mid = lo + ((hi - lo) >> 1)
+        return np.float32(impl(lo, mid) + impl(mid + 1, hi))
+    return impl(1, len(x))
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 15, 16, 17, 1024, 1025, 2048, 2049, 3000, 8195, 12289])
+def test_pairwise_sum32_matches_literal_recursion(oracle, n):
+    rng = np.random.default_rng(n)
+    x = rng.exponential(1.0, n).astype(np.float32) * np.float32(7.3)
+    got = oracle.pairwise_sum32(x)[0]
+    assert got.dtype == np.float32
+    assert got == _julia_pairwise_literal(x)
+    m = np.float32(np.float32(got) / np.float32(n))
+    sq = oracle.pairwise_sum32(x, f=lambda v: np.square((v - m).astype(np.float32)))[0]
+    lit = _julia_pairwise_literal(x, f=lambda v: np.float32(np.float32(v - m) * np.float32(v - m)))
+    assert sq == lit
+
+
+def test_pairwise_leaves_cover_and_split(oracle):
+    for n in [1, 1024, 1025, 5000, 1 << 20, (1 << 20) + 3]:
+        lv = oracle.pairwise_leaves(n)
+        assert lv[0][0] == 0 and lv[-1][1] == n
+        assert all(a[1] == b[0] for a, b in zip(lv, lv[1:]))
+        assert all(1 <= b - a <= 1024 for a, b in lv)
+
+
+def test_fdrstats_float32_semantics(oracle):
+    rng = np.random.default_rng(5)
+    M = rng.exponential(1.0, (3000, 5)).astype(np.float32)
+    m, s = oracle.fdrstats(M)
+    assert isinstance(m, np.float32) and isinstance(s, np.float32)
+    assert m == np.float32(_julia_pairwise_literal(M[:, 0]) / np.float32(3000))
+    inv = np.float32(1.0) / np.float32(2999)  # Float32(1 // (n-1))
+    stds = []
+    for j in range(5):
+        mj = np.float32(_julia_pairwise_literal(M[:, j]) / np.float32(3000))
+        ss = _julia_pairwise_literal(M[:, j], f=lambda v: np.float32(np.float32(v - mj) ** 2))
+        stds.append(np.sqrt(np.float32(ss * inv)))
+    assert s == min(stds)
+    # float64 statistics agree to float32 rounding
+    m64, s64 = oracle.fdrstats_f64(M)
+    assert abs(m - m64) <= 4e-7 * m64 and abs(s - s64) <= 4e-7 * s64
+    # the iterable form: m from the first matrix, s the minimum over all columns
+    m2, s2 = oracle.fdrstats([M[:, :2], M[:, 2:4]])
+    assert m2 == m and s2 == min(stds[:4])
+    # NaN in any column makes s NaN
+    M2 = M.copy()
+    M2[7, 3] = np.nan
+    assert np.isnan(oracle.fdrstats(M2)[1])
+
+
+def test_fdrdenormalize_promotion(oracle):
+    m, s = np.float32(1.2345678), np.float32(0.7654321)
+    t32 = oracle.fdrdenormalize(10, m, s)
+    assert isinstance(t32, np.float32)
+    assert t32 == np.float32(np.float32(np.float32(10) * s) + m)
+    t64 = oracle.fdrdenormalize(10.0, m, s)
+    assert isinstance(t64, float) and t64 == 10.0 * float(s) + float(m)
+    # a Float32 element one ulp below the Float32 threshold is not a proto-hit, at it is
+    x = np.array([[np.nextafter(t32, np.float32(-np.inf))], [t32]], dtype=np.float32)
+    assert oracle.findprotohits(x, t32).tolist() == [[1, 0]]
