@@ -80,9 +80,16 @@ def algorithmic_bytes():
     return 4 * NF * NT + 4 * NF * NR
 
 
-# DRAM bytes (read + write) of one fused zdtfdr! call at this workload, summed over its three
-# kernels from one ncu capture (profiles/zdt_kernels_traffic_Nf2e20_Nt16_Nr129.md).
-NCU_TRAFFIC_PER_CALL = 1_676_704_256
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one fused zdtfdr! call at this
+# workload, summed over its three kernels (zdtf_input64, zdtf_czt<512,16>,
+# zdtf_output_tma64<8>) from one ncu capture of this benchmark's plain leg.  ncu cannot run
+# inside the timed process, so the figure is carried here with the capture it came from.
+NCU_TRAFFIC = {
+    "bytes_per_call": 1_676_704_256,
+    "capture": "ncu --set full --clock-control none -k regex:zdtf_ -s 3 -c 3 python bench.py "
+               "--steps 3 --warmup 1 --no-cpu-baseline --no-e2e --no-batched --no-proposal "
+               "--no-fp32-peak --no-taylor --no-ingest --no-mixed",
+}
 
 
 def nominal_flops():
@@ -284,14 +291,28 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_zdt_sample(spec, workers):
-    """One CPU zdtfdr call (oracle port of the reference's stage sequence) -> seconds."""
+def _oracle():
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import fdr_oracle as o
-    ws = o.ZDTWorkspace(spec, R0, DR, NR, workers=workers)
-    t0 = time.perf_counter()
-    ws.zdtfdr(spec)
-    return time.perf_counter() - t0
+    return o
+
+
+def cpu_zdt_sample(spec, workers, kind="threaded", ws=None):
+    """One CPU zdtfdr call -> (seconds, FDR).  kind "threaded": the oracle's threaded
+    restatement of the reference's stage sequence (complex64, per-call Float32 chirp
+    arguments, scipy pocketfft and elementwise stages on `workers` threads); "mirror": the
+    oracle's bit-faithful FP32 mirror (per-component Float32 rounding, elementwise stages
+    single-threaded)."""
+    o = _oracle()
+    if kind == "threaded":
+        ws = ws or o.ThreadedZDT(spec, R0, DR, NR, workers=workers)
+        t0 = time.perf_counter()
+        out = ws.zdtfdr(spec)
+    else:
+        ws = o.ZDTWorkspace(spec, R0, DR, NR, workers=workers)
+        t0 = time.perf_counter()
+        out = ws.zdtfdr(spec)
+    return time.perf_counter() - t0, out
 
 
 def run_reference(args, rank, world):
@@ -299,9 +320,10 @@ def run_reference(args, rank, world):
         return 0
     workers = os.cpu_count() or 1
     spec = synth(1)
+    ws = _oracle().ThreadedZDT(spec, R0, DR, NR, workers=workers)
     for _ in range(max(0, args.warmup)):
-        cpu_zdt_sample(spec, workers)
-    ts = [cpu_zdt_sample(spec, workers) for _ in range(args.steps)]
+        cpu_zdt_sample(spec, workers, ws=ws)
+    ts = [cpu_zdt_sample(spec, workers, ws=ws)[0] for _ in range(args.steps)]
     tot = sum(ts)
     value = NF * NR * args.steps / tot
     line = {
@@ -312,7 +334,9 @@ def run_reference(args, rank, world):
         "config": {"workload": WORKLOAD, "Nf": NF, "Nt": NT, "Nr": NR},
         "cpu_baseline": {"value": value, "unit": "cells/s", "cores": workers, "kind": "port",
                          "sample": "one full zdtfdr call per step (Julia/FFTW reference absent: "
-                                   "scipy pocketfft restatement, same stage order)"},
+                                   "threaded restatement of the same stage order, complex64, "
+                                   "per-call Float32 chirp arguments, scipy pocketfft, all "
+                                   "host threads)"},
         "e2e": {"value": value, "unit": "cells/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -544,13 +568,35 @@ def main():
     fp32_peak = fp32_peak_tflops(torch) if rank == 0 and not args.no_fp32_peak else None
     flops = nominal_flops()
 
-    cpu = None
+    cpu, error = None, None
     if rank == 0 and not args.no_cpu_baseline:
         workers = os.cpu_count() or 1
-        ts = [cpu_zdt_sample(host_specs[0], workers) for _ in range(3)]
+        o = _oracle()
+        tws = o.ThreadedZDT(host_specs[0], R0, DR, NR, workers=workers)
+        cpu_zdt_sample(host_specs[0], workers, ws=tws)  # warm-up
+        ts = [cpu_zdt_sample(host_specs[0], workers, ws=tws)[0] for _ in range(3)]
+        del tws
+        tm, mirror = cpu_zdt_sample(host_specs[0], workers, kind="mirror")
         cpu = {"value": NF * NR / statistics.median(ts), "unit": "cells/s", "cores": workers,
-               "kind": "port", "sample": "3 full zdtfdr calls on the same config (oracle "
-               "restatement, scipy pocketfft, all host threads), median"}
+               "kind": "port", "sample": "3 full zdtfdr calls on the same config (threaded "
+               "restatement of the reference's stage order: complex64, per-call Float32 chirp "
+               "arguments, scipy pocketfft and elementwise stages on all host threads), median",
+               "mirror": {"value": NF * NR / tm, "unit": "cells/s", "cores": workers,
+                          "kind": "port", "sample": "1 call of the bit-faithful FP32 mirror "
+                          "(per-component Float32 rounding, single-threaded elementwise)"}}
+        # the error of the timed plain form, checked against the oracle on the same input
+        fdr.zdtfdr_(dest, ws, specs[0])
+        got = dest.cpu().numpy()
+        cols = list(range(0, NR, 8))
+        truth = o.fdr_truth(host_specs[0], [R0 + j * DR for j in cols])
+        error = {"rel_linf_vs_fp64": o.rel_linf(got[:, cols], truth),
+                 "rel_l2_vs_fp64": o.rel_l2(got[:, cols], truth),
+                 "fp64_columns": cols,
+                 "rel_linf_vs_fp32_mirror": o.rel_linf(got, mirror),
+                 "rel_l2_vs_fp32_mirror": o.rel_l2(got, mirror),
+                 "mirror_columns": "all", "bound_rel_linf": 1e-4,
+                 "definition": "max|a-b| / max|b|; FP64 = exact-phase Fourier-shift sums"}
+        del mirror, got
 
     if rank == 0:
         line = {
@@ -574,7 +620,8 @@ def main():
                             "zdtfdr! with fused findprotohits(snr=10) -> hits to host"},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": NCU_TRAFFIC_PER_CALL,
+                         "frac": achieved / peak, "traffic": NCU_TRAFFIC["bytes_per_call"],
+                         "traffic_capture": NCU_TRAFFIC["capture"],
                          "kernel": "whole ZDT call (all launches of one zdtfdr!)",
                          "algorithmic_bytes": algorithmic_bytes(), "peak_source": peak_src},
             "compute": {"flop_nominal": flops, "achieved_tflops": flops / (ms_step * 1e-3) / 1e12,
@@ -584,6 +631,7 @@ def main():
             "stages_ms": stages,
             "clocks": clk,
             "cpu_baseline": cpu,
+            "error": error,
             "batched": batched,
             "proposal": proposal,
             "taylor": taylor,

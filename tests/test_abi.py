@@ -90,6 +90,39 @@ def test_batchrates_host_matches_oracle(fdr, oracle):
         assert [list(b) for b in mine] == ref
 
 
+# Expected batches worked by hand from src/batchrates.jl:22-60 (not from a transcription):
+# nc = round(r / δ) ties to even; Nrspan = |nc2 - nc1| + 1; Nrb = growNr(Nt, min(Nrb, Nrspan))
+# = nextprod((2,3,5), Nt + Nrb - 1) - Nt + 1; Nr = cld(Nrspan, Nrb) * Nrb; the bonus
+# Nr - Nrspan goes sign(δ)*bonus/2 rounded from zero below nc1 and rounded to zero above
+# nc2; rates nc1//(Nt-1) .. nc2//(Nt-1) in Nr equal steps, Nrb per batch.
+#   (args, Nrb kw) -> [(first, step, length) per batch]
+HAND_BATCHES = [
+    # span -4..4 Hz/s at 1 Hz/s, Nt=16: nc -4..4, Nrspan 9, 16+9-1 = 24 is smooth: Nrb 9, no bonus
+    ((16, 1.0, -4.0, None), 360, [("-4/15", "1/15", 9)]),
+    # 0..21: Nrspan 22, 16+22-1 = 37 -> 40, Nrb 25, bonus 3 (odd): 2 below (from zero), 1 above
+    ((16, 1.0, 0.0, 21.0), 360, [("-2/15", "1/15", 25)]),
+    # the same span with δ < 0: nc1 = round(-0.0) = 0, nc2 = -21; sign -1: -1.5 from zero = -2,
+    # so nc1 = 0 + 2 = 2; -1.5 to zero = -1, so nc2 = -22; the rates descend
+    ((16, -1.0, 0.0, 21.0), 360, [("2/15", "-1/15", 25)]),
+    # -100..100 with Nrb 50: Nrspan 201, 16+50-1 = 65 -> 72, Nrb 57, Nr = cld(201,57)*57 = 228,
+    # bonus 27: 14 below (13.5 from zero), 13 above (13.5 to zero): -114..113 over 15
+    ((16, 1.0, -100.0, 100.0), 50, [("-114/15", "1/15", 57), ("-57/15", "1/15", 57),
+                                    ("0", "1/15", 57), ("57/15", "1/15", 57)]),
+    # r1 > r2 swaps; Nt=32, δ 2 Hz/s: nc -5..5, Nrspan 11, 32+11-1 = 42 -> 45, Nrb 14, bonus 3
+    ((32, 2.0, 10.0, -10.0), 360, [("-7/31", "1/31", 14)]),
+    # ties to even: 2.5 -> 2, 7.5 -> 8; Nrspan 7, 16+7-1 = 22 -> 24, Nrb 9, bonus 2: 1 and 1
+    ((16, 1.0, 2.5, 7.5), 360, [("1/15", "1/15", 9)]),
+]
+
+
+@pytest.mark.parametrize("args,nrb,expected", HAND_BATCHES)
+def test_batchrates_hand_derived(fdr, args, nrb, expected):
+    from fractions import Fraction
+    got = fdr.batchrates(*args, Nrb=nrb)
+    assert [(b.first, b.step, len(b)) for b in got] == \
+        [(Fraction(a), Fraction(s), n) for a, s, n in expected]
+
+
 def test_rate_range_params(fdr):
     rr = fdr.batchrates(16, 1.0, -4.0)[0]
     assert rr.first == rr.start and len(rr) == rr.length
