@@ -32,7 +32,7 @@ constexpr long long kHitTile = (long long)kHitThreads * kHitRounds;  // elements
 // within a thread (G consecutive units), across the CTA (T threads) and across the S CTAs of
 // a column (S partials, combined by the next kernel).
 // ------------------------------------------------------------------------------------
-constexpr int kPwThreads = 128;
+constexpr int kPwThreads = 256;
 constexpr long long kPwLeaf = 1024;
 
 __device__ __forceinline__ const float* pw_column(const float* const* mats, const float* base,
@@ -63,7 +63,9 @@ __device__ __forceinline__ float pw_add4(float v, float4 a, float m) {
   return __fadd_rn(v, pw_f<SQ>(a.w, m));
 }
 
-// Sequential sum of one leaf of len >= 1 elements.
+// Sequential sum of one leaf of len >= 1 elements.  The 16-byte loads run one batch of four
+// ahead of the adds that consume them (software pipelining), so each thread keeps up to
+// eight loads in flight while its dependent chain of adds proceeds in order.
 template <bool SQ>
 __device__ float pw_leaf(const float* __restrict__ p, long long len, float m) {
   float v;
@@ -77,12 +79,22 @@ __device__ float pw_leaf(const float* __restrict__ p, long long len, float m) {
     v = __fadd_rn(v, pw_f<SQ>(a.z, m));
     v = __fadd_rn(v, pw_f<SQ>(a.w, m));
     long long k = 1;
-    for (; k + 8 <= nq; k += 8) {  // eight 16-byte loads in flight, then their 32 adds in order
-      float4 b[8];
+    if (k + 4 <= nq) {
+      float4 cur[4];
 #pragma unroll
-      for (int u = 0; u < 8; ++u) b[u] = __ldg(q + k + u);
+      for (int u = 0; u < 4; ++u) cur[u] = __ldg(q + k + u);
+      k += 4;
+      for (; k + 4 <= nq; k += 4) {
+        float4 nxt[4];
 #pragma unroll
-      for (int u = 0; u < 8; ++u) v = pw_add4<SQ>(v, b[u], m);
+        for (int u = 0; u < 4; ++u) nxt[u] = __ldg(q + k + u);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) v = pw_add4<SQ>(v, cur[u], m);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) cur[u] = nxt[u];
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) v = pw_add4<SQ>(v, cur[u], m);
     }
     for (; k < nq; ++k) v = pw_add4<SQ>(v, __ldg(q + k), m);
     i = nq << 2;
@@ -94,19 +106,15 @@ __device__ float pw_leaf(const float* __restrict__ p, long long len, float m) {
   return v;
 }
 
-// Value of unit u (depth `bits` node) of a column of n elements.
-template <bool SQ>
-__device__ float pw_unit(const float* __restrict__ x, long long n, int bits, long long u, float m) {
-  long long lo = 0, len = n;
+// Range [lo, lo + len) of unit u (the depth-`bits` node) of a column of n elements.
+__device__ __forceinline__ void pw_unit_range(long long n, int bits, long long u, long long& lo,
+                                              long long& len) {
+  lo = 0;
+  len = n;
   for (int b = bits - 1; b >= 0; --b) {
     const long long c = (len + 1) >> 1;
     if ((u >> b) & 1) { lo += c; len -= c; } else { len = c; }
   }
-  if (len <= kPwLeaf) return pw_leaf<SQ>(x + lo, len, m);
-  const long long c = (len + 1) >> 1;
-  const float a = pw_leaf<SQ>(x + lo, c, m);
-  const float b = pw_leaf<SQ>(x + lo + c, len - c, m);
-  return __fadd_rn(a, b);
 }
 
 // Pairwise (perfect binary tree, left + right) combination of S values, S a power of two.
@@ -123,17 +131,19 @@ __device__ __forceinline__ float pw_tree(const float* __restrict__ v, int S) {
   return stk[top];
 }
 
-// grid (S, ncols), block T (a power of two <= kPwThreads): CTA (s, col) combines the units
-// [s*T*G, (s+1)*T*G) of column col into part[col*S + s].  With SQ, f(x) = abs2(x - mean of
-// the column), the mean taken from the first pass's partials part_sum.
+// grid (S, ncols), block max(2*T, 32) threads (T a power of two <= kPwThreads/2): CTA (s, col)
+// combines the units [s*T*G, (s+1)*T*G) of column col into part[col*S + s].  Threads 2i and
+// 2i+1 (adjacent lanes) take the first and second leaf of each of their G units and combine
+// them with one shuffle.  With SQ, f(x) = abs2(x - mean of the column), the mean taken from
+// the first pass's partials part_sum.
 template <bool SQ>
 __global__ void __launch_bounds__(kPwThreads)
 pw_units_kernel(const float* const* __restrict__ mats, const float* __restrict__ base, long long Nf,
-                long long Nrb, int bits, long long G, int S, const float* __restrict__ part_sum,
+                long long Nrb, int bits, int T, long long G, int S, const float* __restrict__ part_sum,
                 float* __restrict__ part) {
   const long long col = blockIdx.y;
   const float* x = pw_column(mats, base, Nf, Nrb, col);
-  __shared__ float red[kPwThreads];
+  __shared__ float red[kPwThreads / 2];
   __shared__ float s_mean;
   float m = 0.f;
   if (SQ) {
@@ -141,19 +151,29 @@ pw_units_kernel(const float* const* __restrict__ mats, const float* __restrict__
     __syncthreads();
     m = s_mean;
   }
-  const long long u0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * G;
+  const int h = threadIdx.x & 1;
+  const bool active = (int)(threadIdx.x >> 1) < T;  // a block of 32 threads may exceed 2T
+  const long long u0 = ((long long)blockIdx.x * T + (threadIdx.x >> 1)) * G;
   float stk[40];
   for (long long k = 0; k < G; ++k) {
-    float a = pw_unit<SQ>(x, Nf, bits, u0 + k, m);
+    long long lo = 0, len = 0;
+    if (active) pw_unit_range(Nf, bits, u0 + k, lo, len);
+    const bool two = len > kPwLeaf;
+    const long long c = two ? (len + 1) >> 1 : len;
+    const long long ln = h ? (two ? len - c : 0) : c;
+    const float v = ln > 0 ? pw_leaf<SQ>(x + lo + (h ? c : 0), ln, m) : 0.f;
+    const float o = __shfl_xor_sync(0xffffffffu, v, 1);
+    float a = h ? o : v;                    // the unit's first leaf
+    if (two) a = __fadd_rn(a, h ? v : o);   // + its second leaf
     int lev = 0;
     while ((k >> lev) & 1) { a = __fadd_rn(stk[lev], a); ++lev; }
     stk[lev] = a;
   }
   int top = 0;
   while ((1LL << top) < G) ++top;
-  red[threadIdx.x] = stk[top];
+  if (h == 0 && active) red[threadIdx.x >> 1] = stk[top];
   __syncthreads();
-  for (int w = blockDim.x >> 1; w >= 1; w >>= 1) {
+  for (int w = T >> 1; w >= 1; w >>= 1) {
     float a = 0.f;
     if ((int)threadIdx.x < w) a = __fadd_rn(red[2 * threadIdx.x], red[2 * threadIdx.x + 1]);
     __syncthreads();
@@ -209,7 +229,7 @@ static PwShape pw_shape(long long n, long long ncols, int smax) {
   PwShape p;
   p.bits = D > 0 ? D - 1 : 0;
   p.M = 1LL << p.bits;
-  p.T = (int)std::min<long long>(kPwThreads, p.M);
+  p.T = (int)std::min<long long>(kPwThreads / 2, p.M);
   long long S = 1;
   const long long target = 4LL * sm_count();
   while (2 * S <= smax && 2 * S * p.T <= p.M && ncols * S < target) S *= 2;
@@ -230,9 +250,10 @@ int pairwise_stats_launch(const float* const* d_mats, const float* base, long lo
   float* part_sum = part;
   float* part_sq = part + ncols * p.S;
   const dim3 grid((unsigned)p.S, (unsigned)ncols);
-  pw_units_kernel<false><<<grid, p.T, 0, s>>>(d_mats, base, Nf, Nrb, p.bits, p.G, p.S, nullptr, part_sum);
+  const int threads = std::max(32, 2 * p.T);  // whole warps: the leaf exchange is a warp shuffle
+  pw_units_kernel<false><<<grid, threads, 0, s>>>(d_mats, base, Nf, Nrb, p.bits, p.T, p.G, p.S, nullptr, part_sum);
   FDR_LAUNCH_CHECK("pw_units_kernel<sum>");
-  pw_units_kernel<true><<<grid, p.T, 0, s>>>(d_mats, base, Nf, Nrb, p.bits, p.G, p.S, part_sum, part_sq);
+  pw_units_kernel<true><<<grid, threads, 0, s>>>(d_mats, base, Nf, Nrb, p.bits, p.T, p.G, p.S, part_sum, part_sq);
   FDR_LAUNCH_CHECK("pw_units_kernel<abs2>");
   pw_finalize_kernel<<<1, 256, 0, s>>>(part_sum, part_sq, ncols, p.S, Nf, snr_mode, snr, d_ms);
   FDR_LAUNCH_CHECK("pw_finalize_kernel");
