@@ -20,6 +20,7 @@ from .batch import ZDTBatch
 from . import proposal
 from . import ingest
 from .ingest import Filterbank, SearchPipeline, write_filterbank
+from .h5 import H5File, H5Filterbank, H5FormatError, write_fbh5
 from .intfdr import intshift, intshift_, intfdr, intfdr_, taylor_shifts, taylorfdr, taylorfdr_
 from .fftfdr import (FFTFDRWorkspace, fftfdr_workspace, fftfdr_workspace_, fdshiftsum,
                      fdshiftsum_, fdshift, fdshift_, fftfdr, fftfdr_)
@@ -29,7 +30,7 @@ from .fdrutils import (create_fdr, fdrstats, fdrnormalize, fdrnormalize_, fdrden
 _lib.load()  # fail loudly at import when the CUDA library is missing
 
 __all__ = [
-    "FDRError", "ingest", "Filterbank", "SearchPipeline", "write_filterbank", "taylor_shifts", "taylorfdr", "taylorfdr_", "CapacityError", "fortran_empty", "fortran_zeros", "as_device_f32",
+    "FDRError", "ingest", "Filterbank", "H5File", "H5Filterbank", "H5FormatError", "write_fbh5", "SearchPipeline", "write_filterbank", "taylor_shifts", "taylorfdr", "taylorfdr_", "CapacityError", "fortran_empty", "fortran_zeros", "as_device_f32",
     "calcNl", "growNr", "estimate_memory", "driftrates", "batchrates", "RateRange",
     "ZDTWorkspace", "input_", "preprocess_", "convolve_", "postprocess_", "output_",
     "zdtfdr_", "zdtfdr_nodest_", "zdtfdr", "zdtfdr_protohits_", "zdtfdr_blocks_",

@@ -144,6 +144,11 @@ SIGNATURES = {
                                 C.POINTER(I64), C.POINTER(F64), P]),
     "fdr_cluster_protohits": (INT, [P, I64, I64, I64, INT, INT, C.POINTER(P), I64, I64, P, P,
                                     I64, C.POINTER(I64), P]),
+    "fdr_lz4_decompress": (INT, [P, I64, P, I64, C.POINTER(I64)]),
+    "fdr_lz4_compress": (INT, [P, I64, P, I64, C.POINTER(I64)]),
+    "fdr_bitshuffle_lz4_decode": (INT, [P, I64, INT, P, I64, C.POINTER(I64), C.POINTER(I64)]),
+    "fdr_bitshuffle_lz4_encode": (INT, [P, I64, INT, I64, P, I64, C.POINTER(I64)]),
+    "fdr_bitunshuffle": (INT, [P, I64, INT, I64, P, P]),
 }
 
 _lib = None

@@ -180,6 +180,12 @@ class SearchPipeline:
         if fb.nsamples - t0 < self.nt:
             raise ValueError("the file holds fewer time steps than the pipeline's Nt")
         results = []
+        if getattr(fb, "decodes_on_device", False):  # HDF5 products: chunks decoded on the device
+            for c in channels:
+                spec = fb.spectrogram(c * self.nfpc, (c + 1) * self.nfpc, ifno, t0, self.nt,
+                                      out=self.dev[0])
+                results.append((c,) + self.search_channel(spec))
+            return results
         cur = torch.cuda.current_stream()
         if channels:
             self._copy(0, self._gather(fb, channels[0], 0, ifno, t0))

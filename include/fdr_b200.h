@@ -409,6 +409,38 @@ int fdr_cluster_protohits(const int64_t* hits, int64_t nhits, int64_t Nf, int64_
                           int64_t* labels, fdr_hit_cluster* clusters, int64_t capacity,
                           int64_t* nclusters, fdr_stream_t stream);
 
+/* ---------------------------------------------------------------------------------- */
+/* HDF5 filterbank ingest: rawspec's products store the (time, IF, channel) float32       */
+/* dataset "data" in chunks filtered by bitshuffle with LZ4 (HDF5 filter 32008), which   */
+/* test/heavytests.jl:11-14 reads through HDF5.jl + H5Zbitshuffle.jl.  These decode such  */
+/* chunks; the HDF5 structure itself is parsed by the host binding.                       */
+/* ---------------------------------------------------------------------------------- */
+/* One LZ4 block (the LZ4 block format, no frame) from host src into host dst.  Malformed
+   input (truncated sequences, offsets of 0 or before the start) or more than dst_capacity
+   bytes of output return FDR_ERR_INVALID_ARGUMENT. */
+int fdr_lz4_decompress(const uint8_t* src, int64_t src_size, uint8_t* dst, int64_t dst_capacity,
+                       int64_t* dst_size);
+/* Greedy LZ4 block encoder (host); dst_capacity >= src_size + src_size/255 + 16. */
+int fdr_lz4_compress(const uint8_t* src, int64_t src_size, uint8_t* dst, int64_t dst_capacity,
+                     int64_t* dst_size);
+/* A bitshuffle+LZ4 chunk (host): its 12-byte header (big-endian uncompressed bytes and block
+   bytes), the LZ4 blocks decompressed into out, which then holds each block's elements still
+   bit-transposed, followed by the raw (elements mod 8) tail; *nbytes receives the
+   uncompressed size, *block_elems the block length in elements (fdr_bitunshuffle's input). */
+int fdr_bitshuffle_lz4_decode(const uint8_t* chunk, int64_t chunk_size, int elem_size, uint8_t* out,
+                              int64_t out_capacity, int64_t* nbytes, int64_t* block_elems);
+/* The inverse (host): bit-transposed blocks of block_elems elements (shuffled, nbytes) into a
+   bitshuffle+LZ4 chunk. */
+int fdr_bitshuffle_lz4_encode(const uint8_t* shuffled, int64_t nbytes, int elem_size,
+                              int64_t block_elems, uint8_t* out, int64_t out_capacity,
+                              int64_t* out_size);
+/* Device: the bit transpose back to elements of nelem elements of elem_size bytes (1, 2, 4
+   or 8) in blocks of block_elems (a multiple of 8; the last block holds the remaining whole
+   groups of 8, the final nelem mod 8 elements are copied raw).  in and out are device
+   buffers of nelem*elem_size bytes. */
+int fdr_bitunshuffle(const uint8_t* in, int64_t nelem, int elem_size, int64_t block_elems,
+                     uint8_t* out, fdr_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -898,3 +898,96 @@ class ThreadedZDT:
             Y[a:b, :Nr] *= cispi32(postphase_arg(k, lr, self.dr, Nf))
         self._par(post)
         return f.irfft(Y[:, :Nr], n=Nf, axis=0, **w).astype(np.float32, copy=False)  # output!
+
+
+# ----------------------------------------------------------------------------------------
+# Bitshuffle/LZ4 chunks of rawspec's HDF5 products (test/heavytests.jl:11-14 reads them
+# through HDF5.jl + H5Zbitshuffle.jl; the filter is a third-party dependency, restated here
+# from the published bitshuffle and LZ4 block formats)
+# ----------------------------------------------------------------------------------------
+
+def lz4_block_decode(src):
+    """LZ4 block format: sequences of a token (high nibble literal count, low nibble match
+    length - 4, each 15 extended by following bytes until one is < 255), the literals, then
+    (except for the last sequence) a 2-byte little-endian offset back into the output and a
+    copy of the match length, byte by byte so that overlapping copies repeat."""
+    src = bytes(src)
+    out = bytearray()
+    ip = 0
+    while ip < len(src):
+        tok = src[ip]
+        ip += 1
+        lit = tok >> 4
+        if lit == 15:
+            while True:
+                b = src[ip]
+                ip += 1
+                lit += b
+                if b != 255:
+                    break
+        out += src[ip:ip + lit]
+        ip += lit
+        if ip >= len(src):
+            break
+        off = src[ip] | (src[ip + 1] << 8)
+        ip += 2
+        if off == 0 or off > len(out):
+            raise ValueError("lz4: bad offset")
+        ml = tok & 15
+        if ml == 15:
+            while True:
+                b = src[ip]
+                ip += 1
+                ml += b
+                if b != 255:
+                    break
+        ml += 4
+        for _ in range(ml):
+            out.append(out[-off])
+    return bytes(out)
+
+
+def bitshuffle_block(data, elem_size):
+    """Bit transpose of one block of n elements (n a multiple of 8): output bit-row
+    8*j + k (byte j of the little-endian element, bit k, least significant first) holds bit
+    k of byte j of every element, element e at bit (e mod 8) of byte e // 8 of the row."""
+    a = np.frombuffer(bytes(data), dtype=np.uint8).reshape(-1, elem_size)   # (n, es)
+    bits = np.unpackbits(a, axis=1, bitorder="little").reshape(-1, elem_size, 8)  # (n, j, k)
+    rows = bits.transpose(1, 2, 0).reshape(elem_size * 8, -1)               # (8j+k, n)
+    return np.packbits(rows, axis=1, bitorder="little").tobytes()
+
+
+def bitunshuffle_block(data, elem_size):
+    """Inverse of ``bitshuffle_block``."""
+    rows = np.frombuffer(bytes(data), dtype=np.uint8).reshape(elem_size * 8, -1)
+    bits = np.unpackbits(rows, axis=1, bitorder="little")                   # (8j+k, n)
+    n = bits.shape[1]
+    b = bits.reshape(elem_size, 8, n).transpose(2, 0, 1)                    # (n, j, k)
+    return np.packbits(b, axis=2, bitorder="little").reshape(n * elem_size).tobytes()
+
+
+def bitshuffle_lz4_decode_chunk(chunk, elem_size):
+    """A bitshuffle+LZ4 chunk to its elements' bytes: 8-byte big-endian uncompressed size,
+    4-byte big-endian block size in bytes, then per block (the last one holding the
+    remaining whole groups of 8 elements) a 4-byte big-endian compressed size and an LZ4
+    block of bit-transposed elements, then the remaining (elements mod 8) elements raw."""
+    chunk = bytes(chunk)
+    total = int.from_bytes(chunk[0:8], "big")
+    bbytes = int.from_bytes(chunk[8:12], "big")
+    nelem = total // elem_size
+    bel = bbytes // elem_size
+    whole = nelem - nelem % 8
+    ip, out = 12, bytearray()
+    e0 = 0
+    while e0 < whole:
+        ne = min(bel, whole - e0)
+        csz = int.from_bytes(chunk[ip:ip + 4], "big")
+        ip += 4
+        blk = lz4_block_decode(chunk[ip:ip + csz])
+        if len(blk) != ne * elem_size:
+            raise ValueError("bitshuffle: block size mismatch")
+        out += bitunshuffle_block(blk, elem_size)
+        ip += csz
+        e0 += ne
+    out += chunk[ip:ip + (nelem - whole) * elem_size]
+    return bytes(out)
