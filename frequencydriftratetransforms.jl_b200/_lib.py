@@ -9,7 +9,9 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libfdrb200.so")
+# FDR_B200_DEBUG=1 loads the debug build (index checks recorded in device fault words)
+LIB_PATH = os.path.join(HERE, "libfdrb200_debug.so" if os.environ.get("FDR_B200_DEBUG") == "1"
+                        else "libfdrb200.so")
 
 # status codes (fdr_status)
 FDR_OK = 0
@@ -85,6 +87,8 @@ SIGNATURES = {
     "fdr_kernel_launches": (I64, []),
     "fdr_synchronize": (INT, [P]),
     "fdr_selftest_bounded_wait": (INT, [I64, P]),
+    "fdr_debug_build": (INT, []),
+    "fdr_debug_fault": (INT, [C.POINTER(C.c_uint64), P]),
     "fdr_calc_nl": (I64, [I64, I64, C.POINTER(I64), INT]),
     "fdr_grow_nr": (I64, [I64, I64, C.POINTER(I64), INT]),
     "fdr_estimate_memory": (I64, [I64, I64, I64, I64, I64, C.POINTER(I64), INT]),

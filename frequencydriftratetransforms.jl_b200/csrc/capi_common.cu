@@ -16,6 +16,30 @@ static std::atomic<long long> g_launches{0};
 
 void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
+// Readers of the debug builds' per-file fault words (registered by static initialisers).
+static std::vector<int (*)(unsigned long long*)>& debug_readers() {
+  static std::vector<int (*)(unsigned long long*)> v;
+  return v;
+}
+static std::mutex g_debug_mu;
+
+void register_debug_reader(int (*take)(unsigned long long*)) {
+  std::lock_guard<std::mutex> lock(g_debug_mu);
+  debug_readers().push_back(take);
+}
+
+int debug_take_fault(unsigned long long* word) {
+  std::lock_guard<std::mutex> lock(g_debug_mu);
+  unsigned long long first = 0;
+  for (auto fn : debug_readers()) {
+    unsigned long long w = 0;
+    fn(&w);
+    if (w && !first) first = w;
+  }
+  *word = first;
+  return FDR_OK;
+}
+
 void set_error(int status, const char* fmt, ...) {
   char buf[1024];
   va_list ap;
@@ -153,7 +177,37 @@ int fdr_synchronize(fdr_stream_t stream) {
   } else {
     FDR_CUDA(cudaDeviceSynchronize());
   }
-  return fdr::fused_take_fault();
+  const int st = fdr::fused_take_fault();
+  if (st != FDR_OK) return st;
+  unsigned long long w = 0;
+  fdr::debug_take_fault(&w);
+  if (w) {
+    fdr::set_error(FDR_ERR_CUDA, "debug index check failed (source unit %u, line %u)",
+                   (unsigned)((w >> 32) & 0x7fffffffu), (unsigned)(w & 0xffffffffu));
+    return FDR_ERR_CUDA;
+  }
+  return FDR_OK;
+}
+
+int fdr_debug_build(void) {
+#ifdef FDR_DEBUG
+  return 1;
+#else
+  return 0;
+#endif
+}
+
+int fdr_debug_fault(uint64_t* word, fdr_stream_t stream) {
+  FDR_CHECK_ARG(word != nullptr, "fdr_debug_fault: NULL argument");
+  if (stream) {
+    FDR_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+  } else {
+    FDR_CUDA(cudaDeviceSynchronize());
+  }
+  unsigned long long w = 0;
+  fdr::debug_take_fault(&w);
+  *word = (uint64_t)w;
+  return FDR_OK;
 }
 
 int64_t fdr_calc_nl(int64_t Nt, int64_t Nr, const int64_t* factors, int nfactors) {

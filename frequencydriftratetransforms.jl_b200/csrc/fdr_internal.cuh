@@ -48,6 +48,50 @@ void count_launch(int n = 1);
   } while (0)
 
 // ------------------------------------------------------------------------------------
+// Debug build (-DFDR_DEBUG, libfdrb200_debug.so): FDR_DBG_OK(cond) guards a device memory
+// access; a false condition records the first violation of the translation unit (its
+// FDR_TU_ID and source line) in a device word and the access is skipped.  fdr_synchronize
+// reads and clears every unit's word and reports a violation as FDR_ERR_CUDA.  In the
+// normal build FDR_DBG_OK(cond) is `true` and costs nothing.
+// ------------------------------------------------------------------------------------
+void register_debug_reader(int (*take)(unsigned long long*));
+int debug_take_fault(unsigned long long* word);  // first recorded violation, 0 if none
+#ifndef FDR_TU_ID
+#define FDR_TU_ID 0
+#endif
+#ifdef FDR_DEBUG
+namespace dbg {
+static __device__ unsigned long long fault_word;
+static int take(unsigned long long* out) {
+  unsigned long long w = 0;
+  if (cudaMemcpyFromSymbol(&w, fault_word, sizeof(w)) != cudaSuccess) {
+    (void)cudaGetLastError();
+    *out = 0;
+    return 0;
+  }
+  if (w) {
+    const unsigned long long z = 0;
+    (void)cudaMemcpyToSymbol(fault_word, &z, sizeof(z));
+  }
+  *out = w;
+  return 0;
+}
+struct Registration {
+  Registration() { register_debug_reader(&take); }
+};
+static Registration registration;
+__device__ __forceinline__ bool check(bool ok, unsigned line) {
+  if (!ok)
+    atomicCAS(&fault_word, 0ull, (1ull << 63) | ((unsigned long long)FDR_TU_ID << 32) | line);
+  return ok;
+}
+}  // namespace dbg
+#define FDR_DBG_OK(cond) (fdr::dbg::check((cond), __LINE__))
+#else
+#define FDR_DBG_OK(cond) (true)
+#endif
+
+// ------------------------------------------------------------------------------------
 // Complex helpers (float2 = complex64 with .x real, .y imaginary)
 // ------------------------------------------------------------------------------------
 // Complex add / subtract: one packed FP32 add (FADD2) on sm_100 (the same IEEE round-to-nearest

@@ -4,6 +4,7 @@
 #include <math.h>
 #include <string.h>
 
+#define FDR_TU_ID 4
 #include "fdr_internal.cuh"
 
 namespace fdr {
@@ -161,7 +162,7 @@ pw_units_kernel(const float* const* __restrict__ mats, const float* __restrict__
     const bool two = len > kPwLeaf;
     const long long c = two ? (len + 1) >> 1 : len;
     const long long ln = h ? (two ? len - c : 0) : c;
-    const float v = ln > 0 ? pw_leaf<SQ>(x + lo + (h ? c : 0), ln, m) : 0.f;
+    const float v = (ln > 0 && FDR_DBG_OK(lo + (h ? c : 0) + ln <= Nf)) ? pw_leaf<SQ>(x + lo + (h ? c : 0), ln, m) : 0.f;
     const float o = __shfl_xor_sync(0xffffffffu, v, 1);
     float a = h ? o : v;                    // the unit's first leaf
     if (two) a = __fadd_rn(a, h ? v : o);   // + its second leaf
@@ -370,7 +371,7 @@ protohits_write_kernel(const float* const* __restrict__ mats, long long Nf, long
     long long before = running;
     for (int i = 0; i < w; ++i) before += wcount[i];
     before += __popc(bal & ((1u << lane) - 1u));
-    if (hit && before < cap) {
+    if (hit && before < cap && FDR_DBG_OK(before >= 0)) {
       const long long j = e / Nf, i = e - j * Nf;
       hits[2 * before] = i;
       hits[2 * before + 1] = b * Nrb + j;

@@ -17,6 +17,7 @@
 // transpose back to elements runs on the device (fdr_bitunshuffle).
 #include <string.h>
 
+#define FDR_TU_ID 5
 #include "fdr_internal.cuh"
 
 namespace fdr {
@@ -160,7 +161,9 @@ __global__ void bitunshuffle_kernel(const uint8_t* __restrict__ in, long long ne
     for (int j = 0; j < ES; ++j) {
       uint64_t x = 0;
 #pragma unroll
-      for (int k = 0; k < 8; ++k) x |= (uint64_t)src[(8 * j + k) * bg + gi] << (8 * k);
+      for (int k = 0; k < 8; ++k)
+        if (FDR_DBG_OK(b0 * 8 * ES + (8 * j + k) * bg + gi < nelem * ES))
+          x |= (uint64_t)src[(8 * j + k) * bg + gi] << (8 * k);
       x = bit_transpose8(x);  // now byte e = the 8 bits k of element e's byte j
 #pragma unroll
       for (int e = 0; e < 8; ++e) res[e * ES + j] = (uint8_t)(x >> (8 * e));

@@ -8,6 +8,7 @@
 // with n_t = round(rate_j * t) (intfdr.jl:10, ties to even) and indices modulo Nf.
 #include <math.h>
 
+#define FDR_TU_ID 3
 #include "fdr_internal.cuh"
 
 namespace fdr {
@@ -37,7 +38,7 @@ intfdr_kernel(const float* __restrict__ spec, long long Nf, int Nt, int nrates,
         if (n < Nf) {
           long long idx = n + sh;
           if (idx >= Nf) idx -= Nf;
-          acc[v] = __fadd_rn(acc[v], __ldg(col + idx));
+          if (FDR_DBG_OK(idx >= 0 && idx < Nf)) acc[v] = __fadd_rn(acc[v], __ldg(col + idx));
         }
       }
     }
@@ -79,7 +80,7 @@ intfdr_tiled_kernel(const float* __restrict__ spec, long long Nf, int Nt, int nr
     for (int i = threadIdx.x; i < len; i += kIntfdrThreads) {
       long long g = idx + i;
       if (g >= Nf) g -= Nf;  // len <= TN + Nf/4 < Nf: one wrap at most
-      win[tab.off[t] + i] = __ldg(col + g);
+      if (FDR_DBG_OK(g >= 0 && g < Nf && tab.off[t] + i < kTiledMaxWords)) win[tab.off[t] + i] = __ldg(col + g);
     }
   }
   __syncthreads();
@@ -91,7 +92,9 @@ intfdr_tiled_kernel(const float* __restrict__ spec, long long Nf, int Nt, int nr
     for (int t = 0; t < Nt; ++t) {
       const float* w = win + tab.off[t] + tab.rel[jj * Nt + t] + threadIdx.x;
 #pragma unroll
-      for (int v = 0; v < TNV; ++v) acc[v] = __fadd_rn(acc[v], w[v * kIntfdrThreads]);
+      for (int v = 0; v < TNV; ++v)
+        if (FDR_DBG_OK(tab.off[t] + tab.rel[jj * Nt + t] + (int)threadIdx.x + v * kIntfdrThreads < tab.off[t + 1]))
+          acc[v] = __fadd_rn(acc[v], w[v * kIntfdrThreads]);
     }
 #pragma unroll
     for (int v = 0; v < TNV; ++v) {
@@ -109,7 +112,7 @@ __global__ void intshift_kernel(const float* __restrict__ din, long long Nf, int
     const long long t = e / Nf, n = e - t * Nf;
     long long idx = n + tab.sh[t];
     if (idx >= Nf) idx -= Nf;
-    dout[e] = din[idx + t * Nf];
+    if (FDR_DBG_OK(idx >= 0 && idx < Nf)) dout[e] = din[idx + t * Nf];
   }
 }
 

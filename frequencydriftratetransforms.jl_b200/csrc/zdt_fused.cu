@@ -105,8 +105,9 @@ zdtf_input_kernel(const float* __restrict__ spec, long long N, int Nt, int Q,
       const int e = threadIdx.x + i * T;
       const int sp = e % TP, nb = e / TP;
       const long long n = (long long)(na0 + 2 * sp) + (long long)Q * nb;
-      a[i] = __ldcs(reinterpret_cast<const float2*>(c0 + n));
-      b[i] = has1 ? __ldcs(reinterpret_cast<const float2*>(c1 + n)) : make_float2(0.f, 0.f);
+      a[i] = FDR_DBG_OK(n + 2 <= N) ? __ldcs(reinterpret_cast<const float2*>(c0 + n)) : make_float2(0.f, 0.f);
+      b[i] = (has1 && FDR_DBG_OK(n + 2 <= N)) ? __ldcs(reinterpret_cast<const float2*>(c1 + n))
+                                               : make_float2(0.f, 0.f);
     }
 #pragma unroll
     for (int i = 0; i < NL; ++i) {
@@ -123,7 +124,8 @@ zdtf_input_kernel(const float* __restrict__ spec, long long N, int Nt, int Q,
     const int na = na0 + 2 * sp;
     const float2 v0 = cmul(buf[(2 * sp) * SS + pidx(k1)], tw_fwd(tab, (long long)k1 * na));
     const float2 v1 = cmul(buf[(2 * sp + 1) * SS + pidx(k1)], tw_fwd(tab, (long long)k1 * (na + 1)));
-    *reinterpret_cast<float4*>(A + ((long long)p * P + k1) * Q + na) = make_float4(v0.x, v0.y, v1.x, v1.y);
+    if (FDR_DBG_OK(((long long)p * P + k1) * Q + na + 2 <= (long long)gridDim.y * P * Q))
+      *reinterpret_cast<float4*>(A + ((long long)p * P + k1) * Q + na) = make_float4(v0.x, v0.y, v1.x, v1.y);
   }
 }
 
@@ -177,9 +179,9 @@ zdtf_input64_kernel(const float* __restrict__ spec, long long N, int Nt, int Q,
     const long long n0 = (long long)(na0 + seq1) + (long long)Q * nb1;
     const long long st = (long long)Q * P1;
 #pragma unroll
-    for (int m = 0; m < P2; ++m) v[m].x = __ldcs(c0 + n0 + st * m);
+    for (int m = 0; m < P2; ++m) v[m].x = FDR_DBG_OK(n0 + st * m < N) ? __ldcs(c0 + n0 + st * m) : 0.f;
 #pragma unroll
-    for (int m = 0; m < P2; ++m) v[m].y = has1 ? __ldcs(c1 + n0 + st * m) : 0.f;
+    for (int m = 0; m < P2; ++m) v[m].y = (has1 && FDR_DBG_OK(n0 + st * m < N)) ? __ldcs(c1 + n0 + st * m) : 0.f;
   }
   __syncthreads();  // the tables are in shared memory
   Dft<P2>::run(v, -1);
@@ -222,7 +224,8 @@ zdtf_input64_kernel(const float* __restrict__ spec, long long N, int Nt, int Q,
     const int k1 = k1b + P2 * k1a;
     const long long m = (long long)k1 * na;
     const float2 t = cmul(thi[m >> tab.B], tlo[m & (nlo - 1)]);
-    a0[(long long)k1 * Q] = cmul(v[i], t);
+    if (FDR_DBG_OK((long long)p * P * Q + na + (long long)k1 * Q < (long long)gridDim.y * P * Q))
+      a0[(long long)k1 * Q] = cmul(v[i], t);
   }
 }
 // ------------------------------------------------------------------------------------
@@ -278,7 +281,8 @@ __device__ __forceinline__ void czt_forward(const CztArgs& a, int c, const int* 
           const int e = tid + i * T;
           const int seq = e / Q, na = e - seq * Q;
           const int pp = p0 + (seq >> 1), side = seq & 1;
-          v[i] = (pp < a.NP) ? __ldcs(a.A + ((long long)pp * a.P + k1s[side]) * Q + na)
+          v[i] = (pp < a.NP && FDR_DBG_OK(((long long)pp * a.P + k1s[side]) * Q + na < (long long)a.NP * a.P * Q))
+                     ? __ldcs(a.A + ((long long)pp * a.P + k1s[side]) * Q + na)
                              : make_float2(0.f, 0.f);
         }
 #pragma unroll
@@ -518,7 +522,7 @@ __global__ void __launch_bounds__(Q / 2, (Q <= 512 ? 2 : 1)) zdtf_czt_kernel(Czt
     const int k1a = k1s[0], k1b = k1s[1];
     stockham_passes_emit_pp<Q, kRatesPerBlock, SS, T, +1, 1>(hb, ob, twt, [&](int seq, int na, float2 v) {
       const int q = q0 + (seq >> 1), side = seq & 1;
-      if (q < q_end)
+      if (q < q_end && FDR_DBG_OK(((long long)q * P + (side ? k1b : k1a)) * Q + na < (long long)a.npairs * P * Q))
         W[((long long)q * P + (side ? k1b : k1a)) * Q + na] = cmul(v, twr[side * Q + na]);
     });
     if (kFlip) {
@@ -567,7 +571,8 @@ __device__ __forceinline__ void czt_forward_smem(const CztArgs& a, int c, const 
         const int e = tid + i * T;
         const int seq = e / Q, na = e - seq * Q;
         const int pp = p0 + (seq >> 1), side = seq & 1;
-        v[i] = (pp < a.NP) ? __ldcs(a.A + ((long long)pp * a.P + k1s[side]) * Q + na)
+        v[i] = (pp < a.NP && FDR_DBG_OK(((long long)pp * a.P + k1s[side]) * Q + na < (long long)a.NP * a.P * Q))
+                   ? __ldcs(a.A + ((long long)pp * a.P + k1s[side]) * Q + na)
                            : make_float2(0.f, 0.f);
       }
 #pragma unroll
@@ -716,7 +721,7 @@ __global__ void __launch_bounds__(CztSmemShape<Q>::T, 1) zdtf_czt_smem_kernel(Cz
     const int k1a = k1s[0], k1b = k1s[1];
     smem_fft_emit<Q, kRatesPerBlock, SS, T, +1>(buf, twt, [&](int seq, int na, float2 v) {
       const int q = q0 + (seq >> 1), sd = seq & 1;
-      if (q < q_end)
+      if (q < q_end && FDR_DBG_OK(((long long)q * P + (sd ? k1b : k1a)) * Q + na < (long long)a.npairs * P * Q))
         W[((long long)q * P + (sd ? k1b : k1a)) * Q + na] = cmul(v, twr[sd * Q + na]);
     });
   }
@@ -743,7 +748,8 @@ __global__ void __launch_bounds__(CztSmemShape<Q>::T, 1) zdtf_a2f_smem_kernel(Cz
   for (int e = tid; e < Q * a.Nt; e += T) {
     const int t = e / Q, b = e - t * Q;
     const int side = b / (Q / 2), k2 = b - side * (Q / 2);
-    a.F[(long long)k1s[side] + (long long)P * k2 + t * K] = gs[t * Q + b];
+    if (FDR_DBG_OK((long long)k1s[side] + (long long)P * k2 + t * K < K * a.Nt))
+      a.F[(long long)k1s[side] + (long long)P * k2 + t * K] = gs[t * Q + b];
   }
   if (c == 0 && tid == 0)
     for (int t = 0; t < a.Nt; ++t) a.F[a.N / 2 + t * K] = gnyq[t];
@@ -825,8 +831,8 @@ zdtf_output_kernel(const float2* __restrict__ W, long long N, int Q, int Nr, flo
     const long long n = (long long)(na0 + 2 * sp) + (long long)Q * nb;
     const float2 v0 = buf[(2 * sp) * SS + pidx(nb)];
     const float2 v1 = buf[(2 * sp + 1) * SS + pidx(nb)];
-    __stcs(reinterpret_cast<float2*>(d0 + n), make_float2(v0.x, v1.x));
-    if (has1) __stcs(reinterpret_cast<float2*>(d1 + n), make_float2(v0.y, v1.y));
+    if (FDR_DBG_OK(n + 2 <= N && j < Nr)) __stcs(reinterpret_cast<float2*>(d0 + n), make_float2(v0.x, v1.x));
+    if (has1 && FDR_DBG_OK(n + 2 <= N)) __stcs(reinterpret_cast<float2*>(d1 + n), make_float2(v0.y, v1.y));
     if (acc) {
       m[0] += (double)v0.x + (double)v1.x;
       m[1] += (double)v0.x * v0.x + (double)v1.x * v1.x;
@@ -912,8 +918,8 @@ zdtf_output2_kernel(const float2* __restrict__ W, long long N, int Q, int Nr,
 #pragma unroll
     for (int nba = 0; nba < P1; ++nba) {
       const long long off = (long long)Q * P2 * nba;
-      __stcs(d0 + off, v[nba].x);
-      if (has1) __stcs(d1 + off, v[nba].y);
+      if (FDR_DBG_OK(na0 + seq + (long long)Q * r + off < N && j < Nr)) __stcs(d0 + off, v[nba].x);
+      if (has1 && FDR_DBG_OK(na0 + seq + (long long)Q * r + off < N)) __stcs(d1 + off, v[nba].y);
     }
     if (acc) {
 #pragma unroll
@@ -1000,10 +1006,14 @@ __global__ void bounded_wait_selftest_kernel(unsigned long long limit_ns) {
 // both channels of rate j and the odd lane both of rate j + 1 as one 8-byte streaming store
 // each (half the store instructions of per-lane scalar stores).  Every lane of the warp
 // must call it; d0 is this lane's element of rate j, d1 = d0 + Nf.
-__device__ __forceinline__ void store_rate_pair(float* d0, float* d1, float2 v, bool odd, bool has1) {
+__device__ __forceinline__ void store_rate_pair(float* d0, float* d1, float2 v, bool odd, bool has1,
+                                                const float* dlo, const float* dhi) {
   const float recv = __shfl_xor_sync(0xffffffffu, odd ? v.x : v.y, 1);
-  if (!odd) __stcs(reinterpret_cast<float2*>(d0), make_float2(v.x, recv));
-  else if (has1) __stcs(reinterpret_cast<float2*>(d1 - 1), make_float2(recv, v.y));
+  if (!odd) {
+    if (FDR_DBG_OK(d0 >= dlo && d0 + 2 <= dhi)) __stcs(reinterpret_cast<float2*>(d0), make_float2(v.x, recv));
+  } else if (has1) {
+    if (FDR_DBG_OK(d1 - 1 >= dlo && d1 + 1 <= dhi)) __stcs(reinterpret_cast<float2*>(d1 - 1), make_float2(recv, v.y));
+  }
 }
 
 // 2-D tiled TMA load (no multicast) of box {x .. x+15 floats, y .. y+255 rows} into dst.
@@ -1112,7 +1122,7 @@ zdtf_output_tma_kernel(const __grid_constant__ CUtensorMap wmap, long long N, in
 #pragma unroll
       for (int nba = 0; nba < P1; ++nba) {
         const long long off = (long long)Q * P2 * nba;
-        store_rate_pair(d0 + off, d1 + off, w[nba], seq & 1, has1);
+        store_rate_pair(d0 + off, d1 + off, w[nba], seq & 1, has1, dest, dest + N * (long long)Nr);
       }
       if (acc) {
 #pragma unroll
@@ -1265,7 +1275,7 @@ zdtf_output_tma64_kernel(const __grid_constant__ CUtensorMap wmap, long long N, 
       for (int i = 0; i < P1 / 2; ++i) {
         const int nba = (i & (P1 / 4 - 1)) + 16 * h + (i >= P1 / 4 ? P1 / 2 : 0);
         const long long off = (long long)Q * P2 * nba;
-        store_rate_pair(d0 + off, d1 + off, v[i], seq2 & 1, has1);
+        store_rate_pair(d0 + off, d1 + off, v[i], seq2 & 1, has1, dest, dest + N * (long long)Nr);
       }
       if (acc) {
 #pragma unroll
@@ -1504,8 +1514,10 @@ zdtf_output_mma_kernel(const __grid_constant__ CUtensorMap wmap, long long N, in
           const long long n = (long long)(na0 + seq) + (long long)Q * (nbb + 32 * nba);
           const float x0 = c[mt][nt][2 * h], x1 = c[mt][nt][2 * h + 1];
           const float y0 = c[mt + 2][nt][2 * h], y1 = c[mt + 2][nt][2 * h + 1];
-          __stcs(reinterpret_cast<float2*>(dest + (long long)j * N + n), make_float2(x0, x1));
-          if (has1) __stcs(reinterpret_cast<float2*>(dest + (long long)(j + 1) * N + n), make_float2(y0, y1));
+          if (FDR_DBG_OK(n + 2 <= N && j < Nr))
+            __stcs(reinterpret_cast<float2*>(dest + (long long)j * N + n), make_float2(x0, x1));
+          if (has1 && FDR_DBG_OK(n + 2 <= N))
+            __stcs(reinterpret_cast<float2*>(dest + (long long)(j + 1) * N + n), make_float2(y0, y1));
           if (acc) {
             m[0] += (double)x0 + (double)x1;
             m[1] += (double)x0 * x0 + (double)x1 * x1;

@@ -98,6 +98,16 @@ int64_t fdr_kernel_launches(void);
    (NULL: the whole device).  Also reports, once, a bounded wait of the TMA-fed kernels that
    ran out since the last call (FDR_ERR_CUDA; that call's FDR is incomplete). */
 int fdr_synchronize(fdr_stream_t stream);
+/* Debug build (no counterpart in the reference): libfdrb200_debug.so is compiled with
+   FDR_DEBUG, in which the kernels check their global-memory indices against the buffers'
+   extents; a failed check skips the access and records the first violation per source
+   unit (unit id and line), which fdr_synchronize reports as FDR_ERR_CUDA.
+   fdr_debug_build() is 1 in that library, 0 in libfdrb200.so.  fdr_debug_fault synchronises
+   `stream` (NULL: the device) and returns, then clears, the first recorded violation in
+   *word (bit 63 set, unit id in bits 32..62, line in bits 0..31; 0 if none or in the
+   normal build). */
+int fdr_debug_build(void);
+int fdr_debug_fault(uint64_t* word, fdr_stream_t stream);
 /* Self-test of that failure path (no counterpart in the reference): launches one CTA that
    waits on an mbarrier nothing completes, gives up after limit_ns (<= 1 s) and raises the
    fault flag, so that the next fdr_synchronize returns FDR_ERR_CUDA.  No GPU fault. */

@@ -46,3 +46,18 @@ def golden():
     import json
     with open(os.path.join(ROOT, "tests", "golden", "runtests_known_answers.json")) as fh:
         return json.load(fh)
+
+
+@pytest.fixture(autouse=True)
+def _no_debug_index_violation(request):
+    """Under the debug build (FDR_B200_DEBUG=1) every GPU test must end without a recorded
+    index-check violation."""
+    yield
+    if os.environ.get("FDR_B200_DEBUG") != "1" or "gpu" not in request.keywords or not _has_gpu():
+        return
+    import ctypes as C
+    lib = entry.load_package()._lib.lib()
+    assert lib.fdr_debug_build() == 1
+    w = C.c_uint64()
+    assert lib.fdr_debug_fault(C.byref(w), None) == 0
+    assert w.value == 0, f"index check failed: unit {(w.value >> 32) & 0x7fffffff}, line {w.value & 0xffffffff}"

@@ -222,3 +222,13 @@ def test_bounded_wait_fault_is_reported(fdr, oracle):
     truth = oracle.fdr_truth(spec, [-4.0, -3.5])
     assert oracle.rel_linf(out[:, [0, 8]], truth) < 1e-5
     fdr.fdrsynchronize()
+
+
+@pytest.mark.parametrize("Nf,Nt,Nr,staged", [(1 << 12, 16, 33, False), (1 << 12, 65, 33, False),
+                                            (1 << 12, 16, 33, True), (3000, 16, 9, False),
+                                            (1 << 20, 16, 129, False)])
+def test_workspace_path_matches_fused_split(fdr, oracle, Nf, Nt, Nr, staged):
+    """A workspace runs the fused kernels exactly when the host planner returns a split."""
+    spec, _ = oracle.synth_spectrogram(Nf, Nt, 1, 20.0, 20.0, 2.0, seed=Nf + Nt)
+    ws = fdr.ZDTWorkspace(spec, -2.0, 1 / 16, Nr, staged_only=staged)
+    assert ws.fused == (fdr.fused_split(Nf, Nt, Nr, staged_only=staged) is not None)
