@@ -107,6 +107,43 @@ __device__ float pw_leaf(const float* __restrict__ p, long long len, float m) {
   return v;
 }
 
+// Coalesced form for columns whose leaves are all exactly 1024 elements (n a power of two,
+// n >= 2^15, 16-byte aligned columns): leaf i of the column is elements [1024 i, 1024 i +
+// 1024).  The 32 lanes of a warp own 32 leaves; in each of 32 rounds the warp reads 32
+// elements of every one of them with 16-byte loads (four leaves per load instruction, one
+// whole 128-byte line each) into shared memory, then each lane adds its leaf's 32 elements
+// in order.  stage: 32 rows of 33 floats (lane L reading row L, element e, hits bank
+// (L + e) mod 32).
+template <bool SQ>
+__device__ float pw_leaf_warp(const float* __restrict__ x, long long my_leaf, float m,
+                              float* __restrict__ stage) {
+  const int lane = threadIdx.x & 31;
+  const int g = lane >> 3, q = lane & 7;
+  long long slot_leaf[8];  // load i: lanes 8g..8g+7 fetch the leaf of lane 4i + g
+#pragma unroll
+  for (int i = 0; i < 8; ++i) slot_leaf[i] = __shfl_sync(0xffffffffu, my_leaf, 4 * i + g);
+  float v = 0.f;
+  for (int r = 0; r < 32; ++r) {
+    float4 t[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+      t[i] = __ldg(reinterpret_cast<const float4*>(x + slot_leaf[i] * 1024 + 32 * r) + q);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      float* d = stage + (4 * i + g) * 33 + 4 * q;
+      d[0] = t[i].x; d[1] = t[i].y; d[2] = t[i].z; d[3] = t[i].w;
+    }
+    __syncwarp();
+    const float* src = stage + lane * 33;
+    int e0 = 0;
+    if (r == 0) { v = pw_f<SQ>(src[0], m); e0 = 1; }
+#pragma unroll 8
+    for (int e = e0; e < 32; ++e) v = __fadd_rn(v, pw_f<SQ>(src[e], m));
+    __syncwarp();
+  }
+  return v;
+}
+
 // Range [lo, lo + len) of unit u (the depth-`bits` node) of a column of n elements.
 __device__ __forceinline__ void pw_unit_range(long long n, int bits, long long u, long long& lo,
                                               long long& len) {
@@ -141,10 +178,14 @@ template <bool SQ>
 __global__ void __launch_bounds__(kPwThreads)
 pw_units_kernel(const float* const* __restrict__ mats, const float* __restrict__ base, long long Nf,
                 long long Nrb, int bits, int T, long long G, int S, const float* __restrict__ part_sum,
-                float* __restrict__ part) {
+                float* __restrict__ part, int leaves1024) {
   const long long col = blockIdx.y;
   const float* x = pw_column(mats, base, Nf, Nrb, col);
   __shared__ float red[kPwThreads / 2];
+  __shared__ float stage[kPwThreads / 32][32 * 33];
+  // the coalesced form needs every lane active and an aligned column (uniform per CTA)
+  const bool warp_path = leaves1024 && (reinterpret_cast<uintptr_t>(x) & 15) == 0 &&
+                         (int)blockDim.x == 2 * T;
   __shared__ float s_mean;
   float m = 0.f;
   if (SQ) {
@@ -162,7 +203,13 @@ pw_units_kernel(const float* const* __restrict__ mats, const float* __restrict__
     const bool two = len > kPwLeaf;
     const long long c = two ? (len + 1) >> 1 : len;
     const long long ln = h ? (two ? len - c : 0) : c;
-    const float v = (ln > 0 && FDR_DBG_OK(lo + (h ? c : 0) + ln <= Nf)) ? pw_leaf<SQ>(x + lo + (h ? c : 0), ln, m) : 0.f;
+    float v;
+    if (warp_path) {  // unit u = leaves 2u and 2u + 1 of 1024 elements
+      const long long my = 2 * (u0 + k) + h;
+      v = pw_leaf_warp<SQ>(x, FDR_DBG_OK(my * 1024 + 1024 <= Nf) ? my : 0, m, stage[threadIdx.x >> 5]);
+    } else {
+      v = (ln > 0 && FDR_DBG_OK(lo + (h ? c : 0) + ln <= Nf)) ? pw_leaf<SQ>(x + lo + (h ? c : 0), ln, m) : 0.f;
+    }
     const float o = __shfl_xor_sync(0xffffffffu, v, 1);
     float a = h ? o : v;                    // the unit's first leaf
     if (two) a = __fadd_rn(a, h ? v : o);   // + its second leaf
@@ -252,9 +299,13 @@ int pairwise_stats_launch(const float* const* d_mats, const float* base, long lo
   float* part_sq = part + ncols * p.S;
   const dim3 grid((unsigned)p.S, (unsigned)ncols);
   const int threads = std::max(32, 2 * p.T);  // whole warps: the leaf exchange is a warp shuffle
-  pw_units_kernel<false><<<grid, threads, 0, s>>>(d_mats, base, Nf, Nrb, p.bits, p.T, p.G, p.S, nullptr, part_sum);
+  // leaves of exactly 1024 elements (n a power of two >= 2^15, at least 16 units per CTA)
+  const int leaves1024 = (is_pow2(Nf) && Nf >= (1LL << 15) && p.T >= 16) ? 1 : 0;
+  pw_units_kernel<false><<<grid, threads, 0, s>>>(d_mats, base, Nf, Nrb, p.bits, p.T, p.G, p.S, nullptr,
+                                                 part_sum, leaves1024);
   FDR_LAUNCH_CHECK("pw_units_kernel<sum>");
-  pw_units_kernel<true><<<grid, threads, 0, s>>>(d_mats, base, Nf, Nrb, p.bits, p.T, p.G, p.S, part_sum, part_sq);
+  pw_units_kernel<true><<<grid, threads, 0, s>>>(d_mats, base, Nf, Nrb, p.bits, p.T, p.G, p.S, part_sum,
+                                                part_sq, leaves1024);
   FDR_LAUNCH_CHECK("pw_units_kernel<abs2>");
   pw_finalize_kernel<<<1, 256, 0, s>>>(part_sum, part_sq, ncols, p.S, Nf, snr_mode, snr, d_ms);
   FDR_LAUNCH_CHECK("pw_finalize_kernel");
