@@ -7,6 +7,7 @@ torch tensor of shape (Nf, Nt) with strides (1, Nf) ("Fortran order"); indexing
 from __future__ import annotations
 
 import ctypes as C
+import threading
 
 import numpy as np
 import torch
@@ -15,6 +16,24 @@ import torch
 def stream_handle(stream=None):
     s = stream if stream is not None else torch.cuda.current_stream()
     return C.c_void_p(s.cuda_stream)
+
+
+_hit_buffers = threading.local()
+
+
+def host_hit_buffer(capacity: int) -> torch.Tensor:
+    """An int64 hit buffer of at least (capacity, 2) in pinned host memory, kept per host
+    thread and reused by the next call (callers copy the hits out before returning).
+    Pinned memory is mapped into the device's address space, so the library's kernels write
+    the hits into it directly: reading them needs no device-to-host copy, which would go
+    through a copy engine and wait behind an unrelated host-to-device transfer in flight (the
+    next spectrogram of a pipeline)."""
+    cap = max(1, int(capacity))
+    buf = getattr(_hit_buffers, "buf", None)
+    if buf is None or buf.shape[0] < cap:
+        buf = torch.empty((cap, 2), dtype=torch.int64, pin_memory=True)
+        _hit_buffers.buf = buf
+    return buf
 
 
 def is_fortran(t: torch.Tensor) -> bool:

@@ -3,6 +3,7 @@
 #include <stdarg.h>
 #include <string.h>
 
+#include <algorithm>
 #include <atomic>
 #include <mutex>
 
@@ -86,6 +87,91 @@ int64_t nextprod(const int64_t* factors, int nfactors, int64_t n) {
   } r{factors, nfactors, n, &best};
   r.go(0, 1);
   return best == INT64_MAX ? -1 : best;
+}
+
+// Small host arrays (matrix pointers, rate blocks) reach the device as kernel parameters, 512
+// bytes per launch, not through a host-to-device copy: such a copy can queue behind a large
+// transfer that the caller has in flight on a copy engine (the next spectrogram of a pipeline),
+// and every kernel after it would wait for that transfer to finish.
+struct WordChunk {
+  uint32_t w[128];
+};
+
+__global__ void store_words_kernel(WordChunk c, int n, uint32_t* __restrict__ dst) {
+  if ((int)threadIdx.x < n) dst[threadIdx.x] = c.w[threadIdx.x];
+}
+
+int upload_words(void* dev, const void* host, size_t bytes, cudaStream_t s) {
+  FDR_CHECK_ARG(bytes % 4 == 0 && (reinterpret_cast<uintptr_t>(dev) & 3) == 0,
+                "upload of %zu bytes: not whole aligned 32-bit words", bytes);
+  const uint32_t* h = static_cast<const uint32_t*>(host);
+  const size_t n = bytes / 4;
+  for (size_t off = 0; off < n; off += 128) {
+    WordChunk c;
+    const int k = (int)std::min<size_t>(128, n - off);
+    memcpy(c.w, h + off, sizeof(uint32_t) * k);
+    store_words_kernel<<<1, 128, 0, s>>>(c, k, static_cast<uint32_t*>(dev) + off);
+    FDR_LAUNCH_CHECK("store_words_kernel");
+  }
+  return FDR_OK;
+}
+
+// Mapped pinned host words for the small results of a call (proto-hit counts, thresholds),
+// one buffer per host thread, grown on demand.  A kernel stores the results there over the
+// bus: a device-to-host copy would again go through a copy engine and wait behind an
+// unrelated host-to-device transfer in flight.
+namespace {
+struct PinnedStaging {
+  void* p = nullptr;
+  void* d = nullptr;
+  size_t n = 0;
+  ~PinnedStaging() {
+    if (p) (void)cudaFreeHost(p);
+  }
+};
+thread_local PinnedStaging t_staging;
+}  // namespace
+
+int pinned_staging(size_t bytes, void** host, void** dev) {
+  if (t_staging.n < bytes) {
+    if (t_staging.p) (void)cudaFreeHost(t_staging.p);
+    t_staging = PinnedStaging();
+    const size_t n = std::max<size_t>(bytes, 256);
+    void* p = nullptr;
+    void* d = nullptr;
+    FDR_CUDA(cudaHostAlloc(&p, n, cudaHostAllocMapped | cudaHostAllocPortable));
+    const cudaError_t e = cudaHostGetDevicePointer(&d, p, 0);
+    if (e != cudaSuccess) {
+      (void)cudaFreeHost(p);
+      return cuda_status(e, "cudaHostGetDevicePointer");
+    }
+    t_staging.p = p;
+    t_staging.d = d;
+    t_staging.n = n;
+  }
+  *host = t_staging.p;
+  *dev = t_staging.d;
+  return FDR_OK;
+}
+
+int device_view(void* p, void** dp, const char* what) {
+  cudaPointerAttributes a;
+  const cudaError_t e = cudaPointerGetAttributes(&a, p);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    set_error(FDR_ERR_INVALID_ARGUMENT, "%s: not a CUDA-accessible pointer", what);
+    return FDR_ERR_INVALID_ARGUMENT;
+  }
+  if (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) {
+    *dp = p;
+    return FDR_OK;
+  }
+  if (a.type == cudaMemoryTypeHost && a.devicePointer != nullptr) {
+    *dp = a.devicePointer;
+    return FDR_OK;
+  }
+  set_error(FDR_ERR_INVALID_ARGUMENT, "%s: neither device memory nor mapped pinned host memory", what);
+  return FDR_ERR_INVALID_ARGUMENT;
 }
 
 // Stream-ordered scratch comes from a memory pool owned by the library, one per device, that

@@ -156,6 +156,15 @@ inline int ilog2(int64_t n) { int l = 0; while ((int64_t(1) << l) < n) ++l; retu
 // Temporary device memory from the stream-ordered pool.
 int scratch_alloc(void** p, size_t bytes, cudaStream_t s);
 void scratch_free(void* p, cudaStream_t s);
+// Stream-ordered store of a small host array (whole 32-bit words) into device memory by
+// kernel parameters (no copy engine).
+int upload_words(void* dev, const void* host, size_t bytes, cudaStream_t s);
+// Per-host-thread mapped pinned buffer of at least `bytes` for the small results of a call,
+// written by kernels through *dev and read through *host after a synchronisation.
+int pinned_staging(size_t bytes, void** host, void** dev);
+// The address kernels use for a caller's buffer: device or managed memory as is, mapped
+// pinned host memory through its device pointer; anything else is FDR_ERR_INVALID_ARGUMENT.
+int device_view(void* p, void** dp, const char* what);
 
 // Current device's SM count (cached per device).
 int sm_count();
@@ -167,11 +176,18 @@ int stats_device(const float* const* d_mats, int64_t nb, int64_t Nf, int64_t Nrb
 // Float32 fdrstats in the reference's pairwise order over nb*Nrb columns (device pointer
 // array d_mats, or the contiguous matrix `base` when d_mats is NULL).  `part` holds
 // 2*ncols*pairwise_stats_parts(Nf, ncols, smax) floats of scratch; d_ms receives m, s and
-// the threshold fdrdenormalize(snr, m, s) (snr_mode FDR_SNR_F64 / FDR_SNR_F32).
+// the threshold fdrdenormalize(snr, m, s) (snr_mode FDR_SNR_F64 / FDR_SNR_F32).  leafmax,
+// when set, receives the maximum of every pairwise leaf (the proto-hit gate).
 int pairwise_stats_parts(long long Nf, long long ncols, int smax);
 int pairwise_stats_launch(const float* const* d_mats, const float* base, long long nb, long long Nf,
                           long long Nrb, float* part, int smax, double* d_ms, int snr_mode,
-                          double snr, cudaStream_t s);
+                          double snr, cudaStream_t s, float* leafmax = nullptr);
+// findprotohits(...; snr=true): fdrstats, the threshold in snr_mode's type (d_ms = m, s,
+// threshold) and the proto-hits, reading again only the leaves whose maximum reaches the
+// threshold.  Synchronises s.
+int snr_protohits_run(const float* const* d_mats, int64_t nb, int64_t Nf, int64_t Nrb, double* d_ms,
+                      int snr_mode, double snr, int64_t* hits, int64_t capacity, int64_t* count,
+                      double* thr_used, cudaStream_t s);
 int moments_accumulate(const float* x, long long Nf, long long ncols, double* acc, cudaStream_t s);
 int stats_finalize_launch(const double* acc, long long ncols, long long Nf, double* d_ms,
                           cudaStream_t s);

@@ -56,25 +56,30 @@ __device__ __forceinline__ float pw_f(float x, float m) {
   return x;
 }
 
+// v + f(a.x) + f(a.y) + f(a.z) + f(a.w) in order; the plain-sum pass (!SQ) also keeps the
+// running maximum mx of the values (fmaxf: a NaN never becomes the maximum).
 template <bool SQ>
-__device__ __forceinline__ float pw_add4(float v, float4 a, float m) {
+__device__ __forceinline__ float pw_add4(float v, float4 a, float m, float& mx) {
+  if (!SQ) mx = fmaxf(mx, fmaxf(fmaxf(a.x, a.y), fmaxf(a.z, a.w)));
   v = __fadd_rn(v, pw_f<SQ>(a.x, m));
   v = __fadd_rn(v, pw_f<SQ>(a.y, m));
   v = __fadd_rn(v, pw_f<SQ>(a.z, m));
   return __fadd_rn(v, pw_f<SQ>(a.w, m));
 }
 
-// Sequential sum of one leaf of len >= 1 elements.  The 16-byte loads run one batch of four
-// ahead of the adds that consume them (software pipelining), so each thread keeps up to
-// eight loads in flight while its dependent chain of adds proceeds in order.
+// Sequential sum of one leaf of len >= 1 elements (and, for !SQ, its maximum in mx, which
+// starts at -inf).  The 16-byte loads run one batch of four ahead of the adds that consume
+// them (software pipelining), so each thread keeps up to eight loads in flight while its
+// dependent chain of adds proceeds in order.
 template <bool SQ>
-__device__ float pw_leaf(const float* __restrict__ p, long long len, float m) {
+__device__ float pw_leaf(const float* __restrict__ p, long long len, float m, float& mx) {
   float v;
   long long i;
   if ((reinterpret_cast<uintptr_t>(p) & 15) == 0 && len >= 4) {
     const float4* q = reinterpret_cast<const float4*>(p);
     const long long nq = len >> 2;
     const float4 a = __ldg(q);
+    if (!SQ) mx = fmaxf(mx, fmaxf(fmaxf(a.x, a.y), fmaxf(a.z, a.w)));
     v = pw_f<SQ>(a.x, m);
     v = __fadd_rn(v, pw_f<SQ>(a.y, m));
     v = __fadd_rn(v, pw_f<SQ>(a.z, m));
@@ -90,20 +95,26 @@ __device__ float pw_leaf(const float* __restrict__ p, long long len, float m) {
 #pragma unroll
         for (int u = 0; u < 4; ++u) nxt[u] = __ldg(q + k + u);
 #pragma unroll
-        for (int u = 0; u < 4; ++u) v = pw_add4<SQ>(v, cur[u], m);
+        for (int u = 0; u < 4; ++u) v = pw_add4<SQ>(v, cur[u], m, mx);
 #pragma unroll
         for (int u = 0; u < 4; ++u) cur[u] = nxt[u];
       }
 #pragma unroll
-      for (int u = 0; u < 4; ++u) v = pw_add4<SQ>(v, cur[u], m);
+      for (int u = 0; u < 4; ++u) v = pw_add4<SQ>(v, cur[u], m, mx);
     }
-    for (; k < nq; ++k) v = pw_add4<SQ>(v, __ldg(q + k), m);
+    for (; k < nq; ++k) v = pw_add4<SQ>(v, __ldg(q + k), m, mx);
     i = nq << 2;
   } else {
-    v = pw_f<SQ>(__ldg(p), m);
+    const float a = __ldg(p);
+    if (!SQ) mx = fmaxf(mx, a);
+    v = pw_f<SQ>(a, m);
     i = 1;
   }
-  for (; i < len; ++i) v = __fadd_rn(v, pw_f<SQ>(__ldg(p + i), m));
+  for (; i < len; ++i) {
+    const float a = __ldg(p + i);
+    if (!SQ) mx = fmaxf(mx, a);
+    v = __fadd_rn(v, pw_f<SQ>(a, m));
+  }
   return v;
 }
 
@@ -116,7 +127,7 @@ __device__ float pw_leaf(const float* __restrict__ p, long long len, float m) {
 // (L + e) mod 32).
 template <bool SQ>
 __device__ float pw_leaf_warp(const float* __restrict__ x, long long my_leaf, float m,
-                              float* __restrict__ stage) {
+                              float* __restrict__ stage, float& mx) {
   const int lane = threadIdx.x & 31;
   const int g = lane >> 3, q = lane & 7;
   long long slot_leaf[8];  // load i: lanes 8g..8g+7 fetch the leaf of lane 4i + g
@@ -139,6 +150,10 @@ __device__ float pw_leaf_warp(const float* __restrict__ x, long long my_leaf, fl
     if (r == 0) { v = pw_f<SQ>(src[0], m); e0 = 1; }
 #pragma unroll 8
     for (int e = e0; e < 32; ++e) v = __fadd_rn(v, pw_f<SQ>(src[e], m));
+    if (!SQ) {
+#pragma unroll 8
+      for (int e = 0; e < 32; ++e) mx = fmaxf(mx, src[e]);
+    }
     __syncwarp();
   }
   return v;
@@ -173,12 +188,14 @@ __device__ __forceinline__ float pw_tree(const float* __restrict__ v, int S) {
 // combines the units [s*T*G, (s+1)*T*G) of column col into part[col*S + s].  Threads 2i and
 // 2i+1 (adjacent lanes) take the first and second leaf of each of their G units and combine
 // them with one shuffle.  With SQ, f(x) = abs2(x - mean of the column), the mean taken from
-// the first pass's partials part_sum.
+// the first pass's partials part_sum.  Without SQ and with leafmax set, the maximum of leaf
+// slot (u, h) (the first or second leaf of unit u; -inf for the absent second leaf of a
+// one-leaf unit) goes to leafmax[col * 2^(bits+1) + 2u + h].
 template <bool SQ>
 __global__ void __launch_bounds__(kPwThreads)
 pw_units_kernel(const float* const* __restrict__ mats, const float* __restrict__ base, long long Nf,
                 long long Nrb, int bits, int T, long long G, int S, const float* __restrict__ part_sum,
-                float* __restrict__ part, int leaves1024) {
+                float* __restrict__ part, int leaves1024, float* __restrict__ leafmax) {
   const long long col = blockIdx.y;
   const float* x = pw_column(mats, base, Nf, Nrb, col);
   __shared__ float red[kPwThreads / 2];
@@ -204,12 +221,15 @@ pw_units_kernel(const float* const* __restrict__ mats, const float* __restrict__
     const long long c = two ? (len + 1) >> 1 : len;
     const long long ln = h ? (two ? len - c : 0) : c;
     float v;
+    float mx = -INFINITY;
     if (warp_path) {  // unit u = leaves 2u and 2u + 1 of 1024 elements
       const long long my = 2 * (u0 + k) + h;
-      v = pw_leaf_warp<SQ>(x, FDR_DBG_OK(my * 1024 + 1024 <= Nf) ? my : 0, m, stage[threadIdx.x >> 5]);
+      v = pw_leaf_warp<SQ>(x, FDR_DBG_OK(my * 1024 + 1024 <= Nf) ? my : 0, m, stage[threadIdx.x >> 5], mx);
     } else {
-      v = (ln > 0 && FDR_DBG_OK(lo + (h ? c : 0) + ln <= Nf)) ? pw_leaf<SQ>(x + lo + (h ? c : 0), ln, m) : 0.f;
+      v = (ln > 0 && FDR_DBG_OK(lo + (h ? c : 0) + ln <= Nf)) ? pw_leaf<SQ>(x + lo + (h ? c : 0), ln, m, mx) : 0.f;
     }
+    if (!SQ && leafmax && active)
+      leafmax[(col << (bits + 1)) + 2 * (u0 + k) + h] = mx;
     const float o = __shfl_xor_sync(0xffffffffu, v, 1);
     float a = h ? o : v;                    // the unit's first leaf
     if (two) a = __fadd_rn(a, h ? v : o);   // + its second leaf
@@ -290,7 +310,7 @@ int pairwise_stats_parts(long long Nf, long long ncols, int smax) { return pw_sh
 
 int pairwise_stats_launch(const float* const* d_mats, const float* base, long long nb, long long Nf,
                           long long Nrb, float* part, int smax, double* d_ms, int snr_mode,
-                          double snr, cudaStream_t s) {
+                          double snr, cudaStream_t s, float* leafmax) {
   const long long ncols = nb * Nrb;
   FDR_CHECK_ARG(ncols <= 65535, "fdrstats: at most 65535 columns in total");
   FDR_CHECK_ARG(smax >= 1 && smax <= (1 << 20), "fdrstats: bad partial count");
@@ -302,10 +322,10 @@ int pairwise_stats_launch(const float* const* d_mats, const float* base, long lo
   // leaves of exactly 1024 elements (n a power of two >= 2^15, at least 16 units per CTA)
   const int leaves1024 = (is_pow2(Nf) && Nf >= (1LL << 15) && p.T >= 16) ? 1 : 0;
   pw_units_kernel<false><<<grid, threads, 0, s>>>(d_mats, base, Nf, Nrb, p.bits, p.T, p.G, p.S, nullptr,
-                                                 part_sum, leaves1024);
+                                                 part_sum, leaves1024, leafmax);
   FDR_LAUNCH_CHECK("pw_units_kernel<sum>");
   pw_units_kernel<true><<<grid, threads, 0, s>>>(d_mats, base, Nf, Nrb, p.bits, p.T, p.G, p.S, part_sum,
-                                                part_sq, leaves1024);
+                                                part_sq, leaves1024, nullptr);
   FDR_LAUNCH_CHECK("pw_units_kernel<abs2>");
   pw_finalize_kernel<<<1, 256, 0, s>>>(part_sum, part_sq, ncols, p.S, Nf, snr_mode, snr, d_ms);
   FDR_LAUNCH_CHECK("pw_finalize_kernel");
@@ -476,8 +496,9 @@ static unsigned grid_1d(long long total) {
 // Device copy of a host array of nb matrix pointers.
 int upload_ptrs(const void* const* host, int64_t nb, void*** dev, cudaStream_t s) {
   FDR_TRY(scratch_alloc((void**)dev, sizeof(void*) * nb, s));
-  FDR_CUDA(cudaMemcpyAsync(*dev, host, sizeof(void*) * nb, cudaMemcpyHostToDevice, s));
-  return FDR_OK;
+  const int st = upload_words(*dev, host, sizeof(void*) * nb, s);
+  if (st != FDR_OK) scratch_free(*dev, s);
+  return st;
 }
 
 // fdrstats in Float32 pairwise order into the device array ms[3] = (m, s, threshold) (no host
@@ -545,6 +566,53 @@ int threshold_launch(const double* d_ms, int snr_mode, double snr, double* d_thr
   return FDR_OK;
 }
 
+// The total and the threshold of a search into mapped pinned host memory.
+__global__ void hits_result_kernel(const long long* __restrict__ d_total, const double* __restrict__ d_thr,
+                                   long long* __restrict__ out) {
+  out[0] = *d_total;
+  if (d_thr) out[1] = __double_as_longlong(*d_thr);
+}
+
+// Common end of the proto-hit searches: checks the launches, reads the total (d_total) and
+// the threshold (d_thr, else thr_host) back, frees the scratch block and reports capacity.
+static int hits_finish(const long long* d_total, double thr_host, const double* d_thr,
+                       int64_t capacity, int64_t* count, double* thr_used, void* scratch,
+                       cudaStream_t s) {
+  int st = FDR_OK;
+  cudaError_t e = cudaPeekAtLastError();
+  if (e != cudaSuccess) st = cuda_status(e, "protohits kernels");
+  long long total = 0;
+  double thr = thr_host;
+  void* hp = nullptr;
+  void* dp = nullptr;
+  if (st == FDR_OK) st = pinned_staging(2 * sizeof(long long), &hp, &dp);
+  if (st == FDR_OK) {
+    hits_result_kernel<<<1, 1, 0, s>>>(d_total, d_thr, static_cast<long long*>(dp));
+    count_launch();
+    e = cudaPeekAtLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) st = cuda_status(e, "findprotohits count");
+  }
+  if (st == FDR_OK) {
+    const volatile long long* h = static_cast<const volatile long long*>(hp);
+    total = h[0];
+    if (d_thr) {
+      const long long bits = h[1];
+      memcpy(&thr, &bits, sizeof(double));
+    }
+  }
+  scratch_free(scratch, s);
+  if (st != FDR_OK) return st;
+  *count = total;
+  if (thr_used) *thr_used = thr;
+  if (total > capacity) {
+    set_error(FDR_ERR_CAPACITY, "findprotohits: %lld hits exceed capacity %lld", total,
+              (long long)capacity);
+    return FDR_ERR_CAPACITY;
+  }
+  return FDR_OK;
+}
+
 // Count, scan and ordered write of the proto-hits of nb device matrices (d_mats: device
 // array of pointers).  Synchronises s; *count receives the total.  *thr_used receives the
 // threshold (read back from d_thr when given).
@@ -555,6 +623,7 @@ int hits_run(const float* const* d_mats, int64_t nb, int64_t Nf, int64_t Nrb, do
   const long long tiles_per_mat = cdiv(per, kHitTile);
   const long long ntiles = tiles_per_mat * nb;
   FDR_CHECK_ARG(ntiles < (1LL << 31), "findprotohits: too many elements");
+  if (capacity > 0) FDR_TRY(device_view(hits, (void**)&hits, "findprotohits: hit buffer"));
   long long* counts = nullptr;  // ntiles counts, ntiles+1 offsets, then the threshold copy
   FDR_TRY(scratch_alloc((void**)&counts, sizeof(long long) * (2 * ntiles + 2), s));
   long long* offsets = counts + ntiles;
@@ -564,28 +633,154 @@ int hits_run(const float* const* d_mats, int64_t nb, int64_t Nf, int64_t Nrb, do
   protohits_write_kernel<<<(unsigned)ntiles, kHitThreads, 0, s>>>(
       d_mats, Nf, Nrb, tiles_per_mat, thr_host, d_thr, offsets, (long long*)hits, capacity);
   count_launch(3);
-  int st = FDR_OK;
-  cudaError_t e = cudaPeekAtLastError();
-  if (e != cudaSuccess) st = cuda_status(e, "protohits kernels");
-  long long total = 0;
-  double thr = thr_host;
-  if (st == FDR_OK) {
-    e = cudaMemcpyAsync(&total, offsets + ntiles, sizeof(long long), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess && d_thr)
-      e = cudaMemcpyAsync(&thr, d_thr, sizeof(double), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) st = cuda_status(e, "findprotohits count");
+  return hits_finish(offsets + ntiles, thr_host, d_thr, capacity, count, thr_used, counts, s);
+}
+
+// ------------------------------------------------------------------------------------
+// Proto-hits after fdrstats (the snr path): the first statistics pass leaves the maximum of
+// every pairwise leaf, so once the threshold is known only the leaves whose maximum reaches
+// it are read again.  Leaf slots are numbered column by column, and within a column in
+// element order (unit u's first leaf is slot 2u, its second 2u + 1), so writing the hits of
+// the slots in slot order gives findall's column-major order.
+// ------------------------------------------------------------------------------------
+constexpr int kSlotThreads = 256;
+
+// Element range [lo, lo + len) of leaf slot `slot` (2u + h) of a column of n elements.
+__device__ __forceinline__ void pw_slot_range(long long n, int bits, long long slot, long long& lo,
+                                              long long& len) {
+  long long ulo, ulen;
+  pw_unit_range(n, bits, slot >> 1, ulo, ulen);
+  const bool two = ulen > kPwLeaf;
+  const long long c = two ? (ulen + 1) >> 1 : ulen;
+  if ((slot & 1) == 0) { lo = ulo; len = c; }
+  else { lo = ulo + c; len = two ? ulen - c : 0; }
+}
+
+// One thread per leaf slot: slot_count = hits in the slot (0 without reading it when its
+// maximum is below the threshold); block_total[block] = the CTA's sum.  A warp counts each
+// of its lanes' gated slots together, 32 consecutive elements per load.
+__global__ void __launch_bounds__(kSlotThreads)
+protohits_slot_count_kernel(const float* const* __restrict__ mats, long long Nf, long long Nrb, int bits,
+                            long long nslots, const double* __restrict__ d_thr,
+                            const float* __restrict__ leafmax, int* __restrict__ slot_count,
+                            long long* __restrict__ block_total) {
+  const long long slot = (long long)blockIdx.x * kSlotThreads + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const double thr = *d_thr;
+  const bool gate = slot < nslots && (double)leafmax[slot] >= thr;
+  unsigned rem = __ballot_sync(0xffffffffu, gate);
+  int mine = 0;
+  while (rem) {
+    const int L = __ffs(rem) - 1;
+    rem &= rem - 1;
+    const long long sl = slot - lane + L;
+    const long long col = sl >> (bits + 1);
+    long long lo, len;
+    pw_slot_range(Nf, bits, sl - (col << (bits + 1)), lo, len);
+    const float* x = pw_column(mats, nullptr, Nf, Nrb, col) + lo;
+    int c = 0;
+    for (long long e = lane; e < len; e += 32)
+      if (FDR_DBG_OK(lo + e < Nf)) c += ((double)x[e] >= thr);
+    c = (int)__reduce_add_sync(0xffffffffu, (unsigned)c);
+    if (lane == L) mine = c;
   }
-  scratch_free(counts, s);
-  if (st != FDR_OK) return st;
-  *count = total;
-  if (thr_used) *thr_used = thr;
-  if (total > capacity) {
-    set_error(FDR_ERR_CAPACITY, "findprotohits: %lld hits exceed capacity %lld", total,
-              (long long)capacity);
-    return FDR_ERR_CAPACITY;
+  if (slot < nslots) slot_count[slot] = mine;
+  const int wsum = (int)__reduce_add_sync(0xffffffffu, (unsigned)mine);
+  __shared__ int wtot[kSlotThreads / 32];
+  if (lane == 0) wtot[threadIdx.x >> 5] = wsum;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long t = 0;
+    for (int i = 0; i < kSlotThreads / 32; ++i) t += wtot[i];
+    block_total[blockIdx.x] = t;
   }
-  return FDR_OK;
+}
+
+// Writes the hits of each slot with slot_count > 0 at block_off[block] + the exclusive sum of
+// the CTA's earlier slot counts, in element order within the slot (a warp ballot per 32
+// elements).  CTAs without hits, or starting past the capacity, return at once.
+__global__ void __launch_bounds__(kSlotThreads)
+protohits_slot_write_kernel(const float* const* __restrict__ mats, long long Nf, long long Nrb, int bits,
+                            long long nslots, const double* __restrict__ d_thr,
+                            const int* __restrict__ slot_count, const long long* __restrict__ block_off,
+                            long long* __restrict__ hits, long long cap) {
+  const long long start = block_off[blockIdx.x];
+  if (block_off[blockIdx.x + 1] == start || start >= cap) return;  // uniform over the CTA
+  const long long slot = (long long)blockIdx.x * kSlotThreads + threadIdx.x;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int cnt = slot < nslots ? slot_count[slot] : 0;
+  int incl = cnt;  // inclusive scan over the warp
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  __shared__ int wtot[kSlotThreads / 32];
+  if (lane == 31) wtot[w] = incl;
+  __syncthreads();
+  long long my_off = start + incl - cnt;
+  for (int i = 0; i < w; ++i) my_off += wtot[i];
+  const double thr = *d_thr;
+  unsigned rem = __ballot_sync(0xffffffffu, cnt > 0);
+  while (rem) {
+    const int L = __ffs(rem) - 1;
+    rem &= rem - 1;
+    const long long sl = slot - lane + L;
+    long long base = __shfl_sync(0xffffffffu, my_off, L);
+    const long long col = sl >> (bits + 1);
+    long long lo, len;
+    pw_slot_range(Nf, bits, sl - (col << (bits + 1)), lo, len);
+    const float* x = pw_column(mats, nullptr, Nf, Nrb, col) + lo;
+    for (long long e0 = 0; e0 < len; e0 += 32) {
+      const long long e = e0 + lane;
+      const bool hit = e < len && FDR_DBG_OK(lo + e < Nf) && (double)x[e] >= thr;
+      const unsigned bal = __ballot_sync(0xffffffffu, hit);
+      const long long pos = base + __popc(bal & ((1u << lane) - 1u));
+      if (hit && pos < cap && FDR_DBG_OK(pos >= 0)) {
+        hits[2 * pos] = lo + e;
+        hits[2 * pos + 1] = col;
+      }
+      base += __popc(bal);
+    }
+  }
+}
+
+// fdrstats (Float32 pairwise) into d_ms = (m, s, threshold), the threshold fdrdenormalize(snr,
+// m, s) in snr_mode's type, then the proto-hits at or above it through the leaf gate.
+// Synchronises s; returns like hits_run.
+int snr_protohits_run(const float* const* d_mats, int64_t nb, int64_t Nf, int64_t Nrb, double* d_ms,
+                      int snr_mode, double snr, int64_t* hits, int64_t capacity, int64_t* count,
+                      double* thr_used, cudaStream_t s) {
+  const long long ncols = nb * Nrb;
+  FDR_CHECK_ARG(ncols <= 65535, "fdrstats: at most 65535 columns in total");
+  const int smax = 256;
+  const PwShape p = pw_shape(Nf, ncols, smax);
+  const long long nslots = ncols * 2 * p.M;
+  const long long nblk = cdiv(nslots, kSlotThreads);
+  FDR_CHECK_ARG(nblk < (1LL << 31), "findprotohits: too many leaves");
+  if (capacity > 0) FDR_TRY(device_view(hits, (void**)&hits, "findprotohits: hit buffer"));
+  // one scratch block: block totals and offsets (int64), partial sums, leaf maxima, slot counts
+  const size_t b_tot = sizeof(long long) * (2 * nblk + 1);
+  const size_t b_part = sizeof(float) * 2 * ncols * p.S;
+  const size_t b_max = sizeof(float) * nslots;
+  const size_t b_cnt = sizeof(int) * nslots;
+  char* buf = nullptr;
+  FDR_TRY(scratch_alloc((void**)&buf, b_tot + b_part + b_max + b_cnt + 64, s));
+  long long* block_total = reinterpret_cast<long long*>(buf);
+  long long* block_off = block_total + nblk;
+  float* part = reinterpret_cast<float*>(buf + ((b_tot + 15) & ~size_t(15)));
+  float* leafmax = part + 2 * ncols * p.S;
+  int* slot_count = reinterpret_cast<int*>(leafmax + nslots);
+  int st = pairwise_stats_launch(d_mats, nullptr, nb, Nf, Nrb, part, smax, d_ms, snr_mode, snr, s,
+                                 leafmax);
+  if (st != FDR_OK) { scratch_free(buf, s); return st; }
+  const double* d_thr = d_ms + 2;
+  protohits_slot_count_kernel<<<(unsigned)nblk, kSlotThreads, 0, s>>>(
+      d_mats, Nf, Nrb, p.bits, nslots, d_thr, leafmax, slot_count, block_total);
+  scan_counts_kernel<<<1, 1024, 0, s>>>(block_total, nblk, block_off);
+  protohits_slot_write_kernel<<<(unsigned)nblk, kSlotThreads, 0, s>>>(
+      d_mats, Nf, Nrb, p.bits, nslots, d_thr, slot_count, block_off, (long long*)hits, capacity);
+  count_launch(3);
+  return hits_finish(block_off + nblk, snr, d_thr, capacity, count, thr_used, buf, s);
 }
 
 }  // namespace fdr
@@ -647,13 +842,15 @@ int fdr_findprotohits(const float* const* fdrs, int64_t nb, int64_t Nf, int64_t 
   FDR_TRY(upload_ptrs((const void* const*)fdrs, nb, &d_mats, s));
   int st = FDR_OK;
   if (snr) {
-    st = scratch_alloc((void**)&d_ms, 3 * sizeof(double), s);
     // fdrdenormalize(snr, fdrs) = snr*s + m with the reference's Float32 m and s
-    if (st == FDR_OK) st = stats_device((const float* const*)d_mats, nb, Nf, Nrb, d_ms, snr, threshold, s);
+    st = scratch_alloc((void**)&d_ms, 3 * sizeof(double), s);
+    if (st == FDR_OK)
+      st = snr_protohits_run((const float* const*)d_mats, nb, Nf, Nrb, d_ms, snr, threshold, hits,
+                             capacity, count, threshold_used, s);
+  } else {
+    st = hits_run((const float* const*)d_mats, nb, Nf, Nrb, threshold, nullptr, hits, capacity,
+                  count, threshold_used, s);
   }
-  if (st == FDR_OK)
-    st = hits_run((const float* const*)d_mats, nb, Nf, Nrb, threshold, snr ? d_ms + 2 : nullptr,
-                  hits, capacity, count, threshold_used, s);
   scratch_free(d_ms, s);
   scratch_free(d_mats, s);
   return st;

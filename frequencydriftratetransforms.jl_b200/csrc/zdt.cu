@@ -469,8 +469,7 @@ static int zdt_execute_blocks(fdr_zdt* ws, const float* spectrogram, const int32
   for (int64_t i = 0; i < nblocks; ++i) base[(size_t)i] = 8 * (int)blocks[i];
   int* d_blk = nullptr;
   FDR_TRY(scratch_alloc((void**)&d_blk, sizeof(int) * nblocks, s));
-  const cudaError_t ce = cudaMemcpyAsync(d_blk, base.data(), sizeof(int) * nblocks, cudaMemcpyHostToDevice, s);
-  int st = ce == cudaSuccess ? FDR_OK : cuda_status(ce, "upload rate blocks");
+  int st = upload_words(d_blk, base.data(), sizeof(int) * nblocks, s);
   zdt_mark(ws, "start", s);
   if (st == FDR_OK && spectrogram) {
     st = fdr_zdt_input(ws, spectrogram, s);
@@ -516,17 +515,18 @@ int fdr_zdtfdr_protohits(fdr_zdt* ws, const float* spectrogram, const float* r0s
   double* d_ms = acc ? acc + (fast ? 2 * ncols : 0) : nullptr;
   void** d_mats = nullptr;
   if (st == FDR_OK) st = upload_ptrs((const void* const*)dests, nbatch, &d_mats, s);
-  if (st == FDR_OK && snr) {
-    if (fast) {
+  if (st == FDR_OK && snr && !fast) {
+    st = snr_protohits_run((const float* const*)d_mats, nbatch, ws->Nf, ws->Nr, d_ms, snr, threshold,
+                           hits, capacity, count, threshold_used, s);
+  } else {
+    if (st == FDR_OK && snr) {
       st = stats_finalize_launch(acc, ncols, ws->Nf, d_ms, s);
       if (st == FDR_OK) st = threshold_launch(d_ms, snr, threshold, d_ms + 2, s);
-    } else {
-      st = stats_device((const float* const*)d_mats, nbatch, ws->Nf, ws->Nr, d_ms, snr, threshold, s);
     }
+    if (st == FDR_OK)
+      st = hits_run((const float* const*)d_mats, nbatch, ws->Nf, ws->Nr, threshold,
+                    snr ? d_ms + 2 : nullptr, hits, capacity, count, threshold_used, s);
   }
-  if (st == FDR_OK)
-    st = hits_run((const float* const*)d_mats, nbatch, ws->Nf, ws->Nr, threshold,
-                  snr ? d_ms + 2 : nullptr, hits, capacity, count, threshold_used, s);
   scratch_free(d_mats, s);
   scratch_free(acc, s);
   return st;
@@ -563,17 +563,18 @@ int fdr_zdtfdr_blocks_protohits(fdr_zdt* ws, const float* spectrogram, const int
   void** d_mats = nullptr;
   float* const dl[1] = {dest};
   if (st == FDR_OK) st = upload_ptrs((const void* const*)dl, 1, &d_mats, s);
-  if (st == FDR_OK && snr) {
-    if (fast) {
+  if (st == FDR_OK && snr && !fast) {
+    st = snr_protohits_run((const float* const*)d_mats, 1, ws->Nf, ncols, d_ms, snr, threshold, hits,
+                           capacity, count, threshold_used, s);
+  } else {
+    if (st == FDR_OK && snr) {
       st = stats_finalize_launch(acc, ncols, ws->Nf, d_ms, s);
       if (st == FDR_OK) st = threshold_launch(d_ms, snr, threshold, d_ms + 2, s);
-    } else {
-      st = stats_device((const float* const*)d_mats, 1, ws->Nf, ncols, d_ms, snr, threshold, s);
     }
+    if (st == FDR_OK)
+      st = hits_run((const float* const*)d_mats, 1, ws->Nf, ncols, threshold,
+                    snr ? d_ms + 2 : nullptr, hits, capacity, count, threshold_used, s);
   }
-  if (st == FDR_OK)
-    st = hits_run((const float* const*)d_mats, 1, ws->Nf, ncols, threshold,
-                  snr ? d_ms + 2 : nullptr, hits, capacity, count, threshold_used, s);
   scratch_free(d_mats, s);
   scratch_free(acc, s);
   return st;

@@ -7,7 +7,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .arrays import as_device_f32, fortran_empty, ptr, stream_handle
+from .arrays import as_device_f32, fortran_empty, host_hit_buffer, ptr, stream_handle
 
 
 def _mats(fdr):
@@ -87,7 +87,7 @@ def findprotohits(fdr, threshold, snr=False, capacity=None, stream=None, return_
     if capacity is None:
         capacity = 1 << 20
     while True:
-        hits = torch.empty((max(1, capacity), 2), dtype=torch.int64, device="cuda")
+        hits = host_hit_buffer(capacity)
         count = C.c_int64()
         thr = C.c_double()
         st = _lib.lib().fdr_findprotohits(_ptr_array(mats), len(mats), Nf, Nrb,
@@ -99,7 +99,7 @@ def findprotohits(fdr, threshold, snr=False, capacity=None, stream=None, return_
             continue
         _lib.check(st)
         break
-    out = hits[: count.value].cpu().numpy()
+    out = hits[: count.value].numpy().copy()
     return (out, thr.value) if return_threshold else out
 
 

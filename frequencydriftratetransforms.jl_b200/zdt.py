@@ -12,7 +12,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .arrays import (as_device_f32, complex_matrix_view, fortran_empty, ptr,
+from .arrays import (as_device_f32, complex_matrix_view, fortran_empty, host_hit_buffer, ptr,
                      stream_handle)
 
 _WINDOWS = {"rect": _lib.FDR_WINDOW_RECT, "hamming": _lib.FDR_WINDOW_HAMMING}
@@ -312,7 +312,7 @@ def zdtfdr_protohits_(dests, ws: ZDTWorkspace, spectrogram=None, *, r0=None, w="
     r0_arr = (C.c_float * n)(*r0s)
     d_arr = (C.c_void_p * n)(*[d.data_ptr() for d in dl])
     cap = (1 << 20) if capacity is None else int(capacity)
-    hits = torch.empty((max(1, cap), 2), dtype=torch.int64, device="cuda")
+    hits = host_hit_buffer(cap)
     count, thr = C.c_int64(), C.c_double()
     st = _lib.lib().fdr_zdtfdr_protohits(ws._h, ptr(spec), r0_arr, n, d_arr, code, ptr(vals),
                                          float(threshold), _lib.snr_mode(threshold, snr),
@@ -326,7 +326,7 @@ def zdtfdr_protohits_(dests, ws: ZDTWorkspace, spectrogram=None, *, r0=None, w="
         out = findprotohits(dl, thr.value, snr=False, capacity=int(count.value), stream=stream)
         return (out, thr.value) if return_threshold else out
     _lib.check(st)
-    out = hits[: count.value].cpu().numpy()
+    out = hits[: count.value].numpy().copy()
     return (out, thr.value) if return_threshold else out
 
 
@@ -371,7 +371,7 @@ def zdtfdr_blocks_protohits_(dest, ws: ZDTWorkspace, spectrogram, blocks, *, w="
         _check_spec(ws, spec)
     code, vals = _window_args(w, ws.K, ws.Nf)
     cap = (1 << 20) if capacity is None else int(capacity)
-    hits = torch.empty((max(1, cap), 2), dtype=torch.int64, device="cuda")
+    hits = host_hit_buffer(cap)
     count, thr = C.c_int64(), C.c_double()
     st = _lib.lib().fdr_zdtfdr_blocks_protohits(ws._h, ptr(spec), barr, nb, ptr(dest), code,
                                                 ptr(vals), float(threshold),
@@ -385,5 +385,5 @@ def zdtfdr_blocks_protohits_(dest, ws: ZDTWorkspace, spectrogram, blocks, *, w="
         out = findprotohits(dest, thr.value, snr=False, capacity=int(count.value), stream=stream)
         return (out, thr.value) if return_threshold else out
     _lib.check(st)
-    out = hits[: count.value].cpu().numpy()
+    out = hits[: count.value].numpy().copy()
     return (out, thr.value) if return_threshold else out

@@ -183,11 +183,12 @@ int fdr_zdt_execute(fdr_zdt* ws, const float* spectrogram, const float* r0s, int
 /* The fused threshold/proto-hit scan: zdtfdr!(dests, ws[, spectrogram]; r0) followed by
    findprotohits(dests, threshold; snr) (zdtfdr.jl:349-378, fdrutils.jl:148-169).  With snr,
    the statistics are fdr_stats's Float32 pairwise values over the dests (two reads of the
-   FDR), or, for a workspace created with FDR_ZDT_FAST_STATS, float64 column moments
-   accumulated while the FDR columns are written (no extra read).  The FDR is then read
-   once more to count the proto-hits (tiles without hits are not re-read by the write
-   pass).  Hits, count and threshold as in fdr_findprotohits (the batches are the hcat'd
-   matrices).  Synchronises `stream`. */
+   FDR; the first also keeps each pairwise leaf's maximum, so that only leaves that can hold
+   a hit are read again for the proto-hits), or, for a workspace created with
+   FDR_ZDT_FAST_STATS, float64 column moments accumulated while the FDR columns are written
+   (no extra read; the FDR is then read once more to count the proto-hits).  Hits, count and
+   threshold as in fdr_findprotohits (the batches are the hcat'd matrices).  Synchronises
+   `stream`. */
 int fdr_zdtfdr_protohits(fdr_zdt* ws, const float* spectrogram, const float* r0s, int64_t nbatch,
                          float* const* dests, int window, const double* custom_window,
                          double threshold, int snr, int64_t* hits, int64_t capacity,
@@ -378,7 +379,9 @@ int fdr_normalize(float* const* fdrs, int64_t nb, int64_t Nf, int64_t Nrb, float
                   fdr_stream_t stream);
 /* findprotohits (fdrutils.jl:148-169) over nb matrices treated as hcat'd: every (i, j)
    with fdr[i, j] >= threshold, in column-major (findall) order, written as ZERO-based
-   int64 pairs hits[2*h] = i, hits[2*h+1] = j (device buffer of 2*capacity int64).
+   int64 pairs hits[2*h] = i, hits[2*h+1] = j (buffer of 2*capacity int64: device memory,
+   or mapped pinned host memory, which the kernels then write directly, with no copy;
+   other host memory is rejected with FDR_ERR_INVALID_ARGUMENT).
    Each float32 element is compared with the float64 threshold (Julia promotes the
    Float32 element for `>=(threshold)` with a Float64 threshold).  snr = FDR_SNR_F64 or
    FDR_SNR_F32 replaces `threshold` by fdrdenormalize(threshold, fdrs) = threshold*s + m

@@ -82,3 +82,74 @@ def test_findprotohits_capacity(fdr, oracle):
     assert np.array_equal(buf.cpu().numpy(), ref[:4])
     # the Python wrapper grows its buffer and retries
     assert len(fdr.findprotohits(g, 0.0, capacity=16)) == 4096 * 5
+
+
+@pytest.mark.parametrize("Nf,Nr", [(1, 3), (2, 2), (15, 4), (17, 5), (1024, 3), (1025, 2),
+                                   (3000, 7), (8195, 3), (12289, 2), (1 << 16, 2), (100003, 2)])
+def test_findprotohits_snr_ragged_lengths(fdr, oracle, Nf, Nr):
+    """The snr search reads again only the pairwise leaves whose maximum reaches the
+    threshold: hit lists equal the oracle's full scan for ragged column lengths, for sparse
+    (snr 2), dense (snr 0.25) and almost-everything (snr -1) thresholds, in both snr types."""
+    rng = np.random.default_rng(Nf * 5 + Nr)
+    a = (rng.exponential(1.0, (Nf, Nr)) * 16).astype(np.float32)
+    g = fdr.as_device_f32(a)
+    for snr in (2.0, 0.25, -1, 2):
+        hits, thr = fdr.findprotohits(g, snr, snr=True, return_threshold=True)
+        ref = oracle.findprotohits(a, snr, snr=True)
+        assert np.array_equal(hits, ref), (snr, len(hits), len(ref))
+        if Nf == 1:
+            assert np.isnan(thr) and len(hits) == 0  # std of one element is NaN
+
+
+def test_findprotohits_snr_nan_column(fdr, oracle):
+    """A NaN anywhere makes its column's std NaN, so the threshold is NaN and nothing is a
+    hit; a NaN inside a leaf never becomes that leaf's maximum."""
+    a = _fdr(oracle, Nf=8192, Nr=4)
+    a[5000, 2] = np.nan
+    g = fdr.as_device_f32(a)
+    hits, thr = fdr.findprotohits(g, 1.0, snr=True, return_threshold=True)
+    assert np.isnan(thr) and len(hits) == 0
+    assert len(oracle.findprotohits(a, 1.0, snr=True)) == 0
+
+
+def test_findprotohits_snr_capacity(fdr, oracle):
+    """With snr and too small a buffer: FDR_ERR_CAPACITY, the true count and threshold, and
+    the first `capacity` hits in order."""
+    a = _fdr(oracle, Nf=3000, Nr=5)
+    g = fdr.as_device_f32(a)
+    lib = fdr._lib.lib()
+    ref = oracle.findprotohits(a, 0.5, snr=True)
+    assert len(ref) > 40
+    buf = torch.empty((40, 2), dtype=torch.int64, device="cuda")
+    cnt, thr = C.c_int64(), C.c_double()
+    ptrs = (C.c_void_p * 1)(g.data_ptr())
+    st = lib.fdr_findprotohits(ptrs, 1, 3000, 5, 0.5, fdr._lib.FDR_SNR_F64,
+                               C.c_void_p(buf.data_ptr()), 40, C.byref(cnt), C.byref(thr), None)
+    assert st == fdr._lib.FDR_ERR_CAPACITY and cnt.value == len(ref)
+    mr, sr = oracle.fdrstats(a)
+    assert thr.value == float(oracle.fdrdenormalize(0.5, mr, sr))
+    assert np.array_equal(buf.cpu().numpy(), ref[:40])
+
+
+def test_hit_buffer_memory_kinds(fdr, oracle):
+    """The hit buffer may be device memory or pinned (mapped) host memory, which the kernels
+    write directly; pageable host memory is rejected before any kernel runs."""
+    a = _fdr(oracle, Nf=4096, Nr=5)
+    g = fdr.as_device_f32(a)
+    lib = fdr._lib.lib()
+    ref = oracle.findprotohits(a, 40.0)
+    ptrs = (C.c_void_p * 1)(g.data_ptr())
+    for mode, thr in ((0, 40.0), (fdr._lib.FDR_SNR_F64, 2.0)):
+        want = ref if mode == 0 else oracle.findprotohits(a, thr, snr=True)
+        pinned = torch.zeros((len(want) + 3, 2), dtype=torch.int64, pin_memory=True)
+        cnt = C.c_int64()
+        st = lib.fdr_findprotohits(ptrs, 1, 4096, 5, thr, mode, C.c_void_p(pinned.data_ptr()),
+                                   len(want) + 3, C.byref(cnt), None, None)
+        assert st == 0 and cnt.value == len(want)
+        assert np.array_equal(pinned[: cnt.value].numpy(), want)
+        pageable = np.zeros((len(want) + 3, 2), dtype=np.int64)
+        st = lib.fdr_findprotohits(ptrs, 1, 4096, 5, thr, mode,
+                                   C.c_void_p(pageable.ctypes.data), len(want) + 3,
+                                   C.byref(cnt), None, None)
+        assert st == fdr._lib.FDR_ERR_INVALID_ARGUMENT
+        assert not pageable.any()
