@@ -192,14 +192,14 @@ __device__ __forceinline__ float pw_tree(const float* __restrict__ v, int S) {
 // slot (u, h) (the first or second leaf of unit u; -inf for the absent second leaf of a
 // one-leaf unit) goes to leafmax[col * 2^(bits+1) + 2u + h].
 template <bool SQ>
-__global__ void __launch_bounds__(kPwThreads)
+__global__ void __launch_bounds__(kPwThreads, 4)  // <= 64 registers: 8 CTAs of 128 threads per SM
 pw_units_kernel(const float* const* __restrict__ mats, const float* __restrict__ base, long long Nf,
                 long long Nrb, int bits, int T, long long G, int S, const float* __restrict__ part_sum,
                 float* __restrict__ part, int leaves1024, float* __restrict__ leafmax) {
   const long long col = blockIdx.y;
   const float* x = pw_column(mats, base, Nf, Nrb, col);
   __shared__ float red[kPwThreads / 2];
-  __shared__ float stage[kPwThreads / 32][32 * 33];
+  extern __shared__ float stage[];  // coalesced form: 32 x 33 floats per warp
   // the coalesced form needs every lane active and an aligned column (uniform per CTA)
   const bool warp_path = leaves1024 && (reinterpret_cast<uintptr_t>(x) & 15) == 0 &&
                          (int)blockDim.x == 2 * T;
@@ -224,7 +224,8 @@ pw_units_kernel(const float* const* __restrict__ mats, const float* __restrict__
     float mx = -INFINITY;
     if (warp_path) {  // unit u = leaves 2u and 2u + 1 of 1024 elements
       const long long my = 2 * (u0 + k) + h;
-      v = pw_leaf_warp<SQ>(x, FDR_DBG_OK(my * 1024 + 1024 <= Nf) ? my : 0, m, stage[threadIdx.x >> 5], mx);
+      v = pw_leaf_warp<SQ>(x, FDR_DBG_OK(my * 1024 + 1024 <= Nf) ? my : 0, m,
+                           stage + (threadIdx.x >> 5) * (32 * 33), mx);
     } else {
       v = (ln > 0 && FDR_DBG_OK(lo + (h ? c : 0) + ln <= Nf)) ? pw_leaf<SQ>(x + lo + (h ? c : 0), ln, m, mx) : 0.f;
     }
@@ -299,8 +300,14 @@ static PwShape pw_shape(long long n, long long ncols, int smax) {
   p.M = 1LL << p.bits;
   p.T = (int)std::min<long long>(kPwThreads / 2, p.M);
   long long S = 1;
+  // At least ~4 CTAs per SM: more CTAs per column first, then smaller CTAs (down to 32
+  // unit pairs), which also spread more evenly over the SMs.
   const long long target = 4LL * sm_count();
-  while (2 * S <= smax && 2 * S * p.T <= p.M && ncols * S < target) S *= 2;
+  while (ncols * S < target && 2 * S <= smax) {
+    if (2 * S * p.T <= p.M) S *= 2;
+    else if (p.T > 32) { p.T /= 2; S *= 2; }
+    else break;
+  }
   p.S = (int)S;
   p.G = p.M / (S * p.T);
   return p;
@@ -321,11 +328,12 @@ int pairwise_stats_launch(const float* const* d_mats, const float* base, long lo
   const int threads = std::max(32, 2 * p.T);  // whole warps: the leaf exchange is a warp shuffle
   // leaves of exactly 1024 elements (n a power of two >= 2^15, at least 16 units per CTA)
   const int leaves1024 = (is_pow2(Nf) && Nf >= (1LL << 15) && p.T >= 16) ? 1 : 0;
-  pw_units_kernel<false><<<grid, threads, 0, s>>>(d_mats, base, Nf, Nrb, p.bits, p.T, p.G, p.S, nullptr,
-                                                 part_sum, leaves1024, leafmax);
+  const size_t smem = leaves1024 ? sizeof(float) * (threads / 32) * 32 * 33 : 0;
+  pw_units_kernel<false><<<grid, threads, smem, s>>>(d_mats, base, Nf, Nrb, p.bits, p.T, p.G, p.S, nullptr,
+                                                    part_sum, leaves1024, leafmax);
   FDR_LAUNCH_CHECK("pw_units_kernel<sum>");
-  pw_units_kernel<true><<<grid, threads, 0, s>>>(d_mats, base, Nf, Nrb, p.bits, p.T, p.G, p.S, part_sum,
-                                                part_sq, leaves1024, nullptr);
+  pw_units_kernel<true><<<grid, threads, smem, s>>>(d_mats, base, Nf, Nrb, p.bits, p.T, p.G, p.S, part_sum,
+                                                   part_sq, leaves1024, nullptr);
   FDR_LAUNCH_CHECK("pw_units_kernel<abs2>");
   pw_finalize_kernel<<<1, 256, 0, s>>>(part_sum, part_sq, ncols, p.S, Nf, snr_mode, snr, d_ms);
   FDR_LAUNCH_CHECK("pw_finalize_kernel");
@@ -414,13 +422,18 @@ protohits_count_kernel(const float* const* __restrict__ mats, long long Nf, long
 }
 
 // Pass 2: write the hits of each tile at offsets[tile], in column-major order.  Tiles
-// without hits return at once, so this pass re-reads only the tiles that hold hits.
+// without hits return at once, so this pass re-reads only the tiles that hold hits.  CTA 0
+// also stores the total and the threshold in result[0..1] (mapped host memory).
 __global__ void __launch_bounds__(kHitThreads)
 protohits_write_kernel(const float* const* __restrict__ mats, long long Nf, long long Nrb,
-                       long long tiles_per_mat, double thr_host, const double* __restrict__ d_thr,
-                       const long long* __restrict__ offsets, long long* __restrict__ hits,
-                       long long cap) {
+                       long long tiles_per_mat, long long ntiles, double thr_host,
+                       const double* __restrict__ d_thr, const long long* __restrict__ offsets,
+                       long long* __restrict__ hits, long long cap, long long* __restrict__ result) {
   const long long tile = blockIdx.x;
+  if (tile == 0 && threadIdx.x == 0) {  // the total and the threshold, for the host
+    result[0] = offsets[ntiles];
+    result[1] = __double_as_longlong(d_thr ? *d_thr : thr_host);
+  }
   const long long start = offsets[tile];
   if (offsets[tile + 1] == start || start >= cap) return;  // uniform over the CTA
   const long long b = tile / tiles_per_mat, tt = tile - b * tiles_per_mat;
@@ -467,24 +480,39 @@ __global__ void threshold_kernel(const double* __restrict__ ms, int snr_mode, do
                                    : snr * (double)s + (double)m;
 }
 
-// Exclusive scan of counts (single CTA); offsets[n] = total.
+// Exclusive scan of counts (single CTA of whole warps); offsets[n] = total.  Each thread sums a
+// contiguous chunk, the chunk sums are scanned with warp shuffles (within and then across the
+// warps), and each thread writes its chunk's offsets.
 __global__ void scan_counts_kernel(const long long* __restrict__ counts, long long n,
                                    long long* __restrict__ offsets) {
-  __shared__ long long part[1024];
+  __shared__ long long wsum[32];
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5, nw = blockDim.x >> 5;
   const long long per = (n + blockDim.x - 1) / blockDim.x;
-  const long long a = threadIdx.x * per, bnd = min(n, a + per);
+  const long long a = min(n, (long long)t * per), bnd = min(n, a + per);
   long long s = 0;
   for (long long i = a; i < bnd; ++i) s += counts[i];
-  part[threadIdx.x] = s;
+  long long x = s;  // inclusive scan over the warp
+  for (int o = 1; o < 32; o <<= 1) {
+    const long long y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wsum[w] = x;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    long long run = 0;
-    for (int i = 0; i < blockDim.x; ++i) { long long v = part[i]; part[i] = run; run += v; }
-    offsets[n] = run;
+  if (w == 0) {
+    long long y = lane < nw ? wsum[lane] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      const long long z = __shfl_up_sync(0xffffffffu, y, o);
+      if (lane >= o) y += z;
+    }
+    wsum[lane] = y;
   }
   __syncthreads();
-  long long run = part[threadIdx.x];
-  for (long long i = a; i < bnd; ++i) { offsets[i] = run; run += counts[i]; }
+  long long run = x - s + (w > 0 ? wsum[w - 1] : 0);
+  if (t == (int)blockDim.x - 1) offsets[n] = run + s;
+  for (long long i = a; i < bnd; ++i) {
+    offsets[i] = run;
+    run += counts[i];
+  }
 }
 
 static unsigned grid_1d(long long total) {
@@ -566,43 +594,23 @@ int threshold_launch(const double* d_ms, int snr_mode, double snr, double* d_thr
   return FDR_OK;
 }
 
-// The total and the threshold of a search into mapped pinned host memory.
-__global__ void hits_result_kernel(const long long* __restrict__ d_total, const double* __restrict__ d_thr,
-                                   long long* __restrict__ out) {
-  out[0] = *d_total;
-  if (d_thr) out[1] = __double_as_longlong(*d_thr);
-}
-
-// Common end of the proto-hit searches: checks the launches, reads the total (d_total) and
-// the threshold (d_thr, else thr_host) back, frees the scratch block and reports capacity.
-static int hits_finish(const long long* d_total, double thr_host, const double* d_thr,
-                       int64_t capacity, int64_t* count, double* thr_used, void* scratch,
-                       cudaStream_t s) {
+// Common end of the proto-hit searches: checks the launches, waits for the stream and reads
+// the total and the threshold that the write kernel stored in the mapped words `h`, frees
+// the scratch block and reports capacity.
+static int hits_finish(const volatile long long* h, bool has_thr, double thr_host, int64_t capacity,
+                       int64_t* count, double* thr_used, void* scratch, cudaStream_t s) {
   int st = FDR_OK;
   cudaError_t e = cudaPeekAtLastError();
-  if (e != cudaSuccess) st = cuda_status(e, "protohits kernels");
-  long long total = 0;
-  double thr = thr_host;
-  void* hp = nullptr;
-  void* dp = nullptr;
-  if (st == FDR_OK) st = pinned_staging(2 * sizeof(long long), &hp, &dp);
-  if (st == FDR_OK) {
-    hits_result_kernel<<<1, 1, 0, s>>>(d_total, d_thr, static_cast<long long*>(dp));
-    count_launch();
-    e = cudaPeekAtLastError();
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) st = cuda_status(e, "findprotohits count");
-  }
-  if (st == FDR_OK) {
-    const volatile long long* h = static_cast<const volatile long long*>(hp);
-    total = h[0];
-    if (d_thr) {
-      const long long bits = h[1];
-      memcpy(&thr, &bits, sizeof(double));
-    }
-  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) st = cuda_status(e, "findprotohits");
   scratch_free(scratch, s);
   if (st != FDR_OK) return st;
+  const long long total = h[0];
+  double thr = thr_host;
+  if (has_thr) {
+    const long long bits = h[1];
+    memcpy(&thr, &bits, sizeof(double));
+  }
   *count = total;
   if (thr_used) *thr_used = thr;
   if (total > capacity) {
@@ -624,6 +632,8 @@ int hits_run(const float* const* d_mats, int64_t nb, int64_t Nf, int64_t Nrb, do
   const long long ntiles = tiles_per_mat * nb;
   FDR_CHECK_ARG(ntiles < (1LL << 31), "findprotohits: too many elements");
   if (capacity > 0) FDR_TRY(device_view(hits, (void**)&hits, "findprotohits: hit buffer"));
+  void *res_host = nullptr, *res_dev = nullptr;
+  FDR_TRY(pinned_staging(2 * sizeof(long long), &res_host, &res_dev));
   long long* counts = nullptr;  // ntiles counts, ntiles+1 offsets, then the threshold copy
   FDR_TRY(scratch_alloc((void**)&counts, sizeof(long long) * (2 * ntiles + 2), s));
   long long* offsets = counts + ntiles;
@@ -631,9 +641,11 @@ int hits_run(const float* const* d_mats, int64_t nb, int64_t Nf, int64_t Nrb, do
                                                                  thr_host, d_thr, counts);
   scan_counts_kernel<<<1, 1024, 0, s>>>(counts, ntiles, offsets);
   protohits_write_kernel<<<(unsigned)ntiles, kHitThreads, 0, s>>>(
-      d_mats, Nf, Nrb, tiles_per_mat, thr_host, d_thr, offsets, (long long*)hits, capacity);
+      d_mats, Nf, Nrb, tiles_per_mat, ntiles, thr_host, d_thr, offsets, (long long*)hits, capacity,
+      static_cast<long long*>(res_dev));
   count_launch(3);
-  return hits_finish(offsets + ntiles, thr_host, d_thr, capacity, count, thr_used, counts, s);
+  return hits_finish(static_cast<const volatile long long*>(res_host), d_thr != nullptr, thr_host,
+                     capacity, count, thr_used, counts, s);
 }
 
 // ------------------------------------------------------------------------------------
@@ -656,57 +668,81 @@ __device__ __forceinline__ void pw_slot_range(long long n, int bits, long long s
   else { lo = ulo + c; len = two ? ulen - c : 0; }
 }
 
+// The elements of a leaf slot (at most 1024) into the lanes' registers: v[i] = x[lane + 32 i].
+// All 32 loads of a lane are issued before any is used, so a slot costs one memory latency.
+__device__ __forceinline__ void slot_load(const float* __restrict__ x, long long lo, long long len,
+                                          long long Nf, int lane, float (&v)[32]) {
+#pragma unroll
+  for (int i = 0; i < 32; ++i) {
+    const long long e = lane + 32 * i;
+    v[i] = (e < len && FDR_DBG_OK(lo + e < Nf)) ? __ldg(x + e) : 0.f;
+  }
+}
+
 // One thread per leaf slot: slot_count = hits in the slot (0 without reading it when its
-// maximum is below the threshold); block_total[block] = the CTA's sum.  A warp counts each
-// of its lanes' gated slots together, 32 consecutive elements per load.
+// maximum is below the threshold); block_total[block] = the CTA's sum.  The CTA's gated
+// slots are listed in shared memory and dealt out to its warps, one slot per warp at a time.
 __global__ void __launch_bounds__(kSlotThreads)
 protohits_slot_count_kernel(const float* const* __restrict__ mats, long long Nf, long long Nrb, int bits,
                             long long nslots, const double* __restrict__ d_thr,
                             const float* __restrict__ leafmax, int* __restrict__ slot_count,
                             long long* __restrict__ block_total) {
-  const long long slot = (long long)blockIdx.x * kSlotThreads + threadIdx.x;
-  const int lane = threadIdx.x & 31;
+  __shared__ int list[kSlotThreads];
+  __shared__ int nlist, total;
+  const long long slot0 = (long long)blockIdx.x * kSlotThreads;
+  const long long slot = slot0 + threadIdx.x;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const double thr = *d_thr;
+  if (threadIdx.x == 0) nlist = total = 0;
+  __syncthreads();
   const bool gate = slot < nslots && (double)leafmax[slot] >= thr;
-  unsigned rem = __ballot_sync(0xffffffffu, gate);
-  int mine = 0;
-  while (rem) {
-    const int L = __ffs(rem) - 1;
-    rem &= rem - 1;
-    const long long sl = slot - lane + L;
+  if (gate) list[atomicAdd(&nlist, 1)] = threadIdx.x;
+  else if (slot < nslots) slot_count[slot] = 0;
+  __syncthreads();
+  for (int k = w; k < nlist; k += kSlotThreads / 32) {
+    const long long sl = slot0 + list[k];
     const long long col = sl >> (bits + 1);
     long long lo, len;
     pw_slot_range(Nf, bits, sl - (col << (bits + 1)), lo, len);
-    const float* x = pw_column(mats, nullptr, Nf, Nrb, col) + lo;
+    float v[32];
+    slot_load(pw_column(mats, nullptr, Nf, Nrb, col) + lo, lo, len, Nf, lane, v);
     int c = 0;
-    for (long long e = lane; e < len; e += 32)
-      if (FDR_DBG_OK(lo + e < Nf)) c += ((double)x[e] >= thr);
+#pragma unroll
+    for (int i = 0; i < 32; ++i) c += (lane + 32 * i < len) && ((double)v[i] >= thr);
     c = (int)__reduce_add_sync(0xffffffffu, (unsigned)c);
-    if (lane == L) mine = c;
+    if (lane == 0) {
+      slot_count[sl] = c;
+      atomicAdd(&total, c);
+    }
   }
-  if (slot < nslots) slot_count[slot] = mine;
-  const int wsum = (int)__reduce_add_sync(0xffffffffu, (unsigned)mine);
-  __shared__ int wtot[kSlotThreads / 32];
-  if (lane == 0) wtot[threadIdx.x >> 5] = wsum;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    long long t = 0;
-    for (int i = 0; i < kSlotThreads / 32; ++i) t += wtot[i];
-    block_total[blockIdx.x] = t;
-  }
+  if (threadIdx.x == 0) block_total[blockIdx.x] = total;
 }
 
 // Writes the hits of each slot with slot_count > 0 at block_off[block] + the exclusive sum of
 // the CTA's earlier slot counts, in element order within the slot (a warp ballot per 32
-// elements).  CTAs without hits, or starting past the capacity, return at once.
+// elements), one 16-byte (i, j) store per hit when the buffer allows (consecutive hits of a
+// ballot land in one contiguous run, which also suits a buffer in mapped host memory).  The
+// CTA's slots with hits are dealt out to its warps.  CTAs without hits, or starting past the
+// capacity, return at once; CTA 0 first stores the total and the threshold in result[0..1].
 __global__ void __launch_bounds__(kSlotThreads)
 protohits_slot_write_kernel(const float* const* __restrict__ mats, long long Nf, long long Nrb, int bits,
-                            long long nslots, const double* __restrict__ d_thr,
+                            long long nslots, long long nblk, const double* __restrict__ d_thr,
                             const int* __restrict__ slot_count, const long long* __restrict__ block_off,
-                            long long* __restrict__ hits, long long cap) {
+                            long long* __restrict__ hits, long long cap, long long* __restrict__ result) {
+  const double thr = *d_thr;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    result[0] = block_off[nblk];
+    result[1] = __double_as_longlong(thr);
+  }
   const long long start = block_off[blockIdx.x];
   if (block_off[blockIdx.x + 1] == start || start >= cap) return;  // uniform over the CTA
-  const long long slot = (long long)blockIdx.x * kSlotThreads + threadIdx.x;
+  __shared__ int wtot[kSlotThreads / 32];
+  __shared__ int list[kSlotThreads];
+  __shared__ long long offs[kSlotThreads];
+  __shared__ int nlist;
+  const long long slot0 = (long long)blockIdx.x * kSlotThreads;
+  const long long slot = slot0 + threadIdx.x;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int cnt = slot < nslots ? slot_count[slot] : 0;
   int incl = cnt;  // inclusive scan over the warp
@@ -714,30 +750,41 @@ protohits_slot_write_kernel(const float* const* __restrict__ mats, long long Nf,
     const int y = __shfl_up_sync(0xffffffffu, incl, o);
     if (lane >= o) incl += y;
   }
-  __shared__ int wtot[kSlotThreads / 32];
   if (lane == 31) wtot[w] = incl;
+  if (threadIdx.x == 0) nlist = 0;
   __syncthreads();
   long long my_off = start + incl - cnt;
   for (int i = 0; i < w; ++i) my_off += wtot[i];
-  const double thr = *d_thr;
-  unsigned rem = __ballot_sync(0xffffffffu, cnt > 0);
-  while (rem) {
-    const int L = __ffs(rem) - 1;
-    rem &= rem - 1;
-    const long long sl = slot - lane + L;
-    long long base = __shfl_sync(0xffffffffu, my_off, L);
+  if (cnt > 0) {
+    const int k = atomicAdd(&nlist, 1);
+    list[k] = threadIdx.x;
+    offs[k] = my_off;
+  }
+  __syncthreads();
+  const bool vec = (reinterpret_cast<uintptr_t>(hits) & 15) == 0;
+  for (int k = w; k < nlist; k += kSlotThreads / 32) {
+    const long long sl = slot0 + list[k];
+    long long base = offs[k];
+    if (base >= cap) continue;  // uniform over the warp
     const long long col = sl >> (bits + 1);
     long long lo, len;
     pw_slot_range(Nf, bits, sl - (col << (bits + 1)), lo, len);
-    const float* x = pw_column(mats, nullptr, Nf, Nrb, col) + lo;
-    for (long long e0 = 0; e0 < len; e0 += 32) {
-      const long long e = e0 + lane;
-      const bool hit = e < len && FDR_DBG_OK(lo + e < Nf) && (double)x[e] >= thr;
+    float v[32];
+    slot_load(pw_column(mats, nullptr, Nf, Nrb, col) + lo, lo, len, Nf, lane, v);
+#pragma unroll
+    for (int i = 0; i < 32; ++i) {
+      const long long e = lane + 32 * i;
+      const bool hit = e < len && (double)v[i] >= thr;
       const unsigned bal = __ballot_sync(0xffffffffu, hit);
+      if (bal == 0u) continue;  // uniform over the warp
       const long long pos = base + __popc(bal & ((1u << lane) - 1u));
       if (hit && pos < cap && FDR_DBG_OK(pos >= 0)) {
-        hits[2 * pos] = lo + e;
-        hits[2 * pos + 1] = col;
+        if (vec) {
+          *reinterpret_cast<longlong2*>(hits + 2 * pos) = make_longlong2(lo + e, col);
+        } else {
+          hits[2 * pos] = lo + e;
+          hits[2 * pos + 1] = col;
+        }
       }
       base += __popc(bal);
     }
@@ -758,6 +805,8 @@ int snr_protohits_run(const float* const* d_mats, int64_t nb, int64_t Nf, int64_
   const long long nblk = cdiv(nslots, kSlotThreads);
   FDR_CHECK_ARG(nblk < (1LL << 31), "findprotohits: too many leaves");
   if (capacity > 0) FDR_TRY(device_view(hits, (void**)&hits, "findprotohits: hit buffer"));
+  void *res_host = nullptr, *res_dev = nullptr;
+  FDR_TRY(pinned_staging(2 * sizeof(long long), &res_host, &res_dev));
   // one scratch block: block totals and offsets (int64), partial sums, leaf maxima, slot counts
   const size_t b_tot = sizeof(long long) * (2 * nblk + 1);
   const size_t b_part = sizeof(float) * 2 * ncols * p.S;
@@ -778,9 +827,11 @@ int snr_protohits_run(const float* const* d_mats, int64_t nb, int64_t Nf, int64_
       d_mats, Nf, Nrb, p.bits, nslots, d_thr, leafmax, slot_count, block_total);
   scan_counts_kernel<<<1, 1024, 0, s>>>(block_total, nblk, block_off);
   protohits_slot_write_kernel<<<(unsigned)nblk, kSlotThreads, 0, s>>>(
-      d_mats, Nf, Nrb, p.bits, nslots, d_thr, slot_count, block_off, (long long*)hits, capacity);
+      d_mats, Nf, Nrb, p.bits, nslots, nblk, d_thr, slot_count, block_off, (long long*)hits, capacity,
+      static_cast<long long*>(res_dev));
   count_launch(3);
-  return hits_finish(block_off + nblk, snr, d_thr, capacity, count, thr_used, buf, s);
+  return hits_finish(static_cast<const volatile long long*>(res_host), true, snr, capacity, count,
+                     thr_used, buf, s);
 }
 
 }  // namespace fdr
