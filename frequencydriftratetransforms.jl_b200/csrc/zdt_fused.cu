@@ -535,20 +535,36 @@ __global__ void __launch_bounds__(Q / 2, (Q <= 512 ? 2 : 1)) zdtf_czt_kernel(Czt
 
 // ------------------------------------------------------------------------------------
 // Kernel B for 16 < Nt <= NT (32 or 64): F[k, t] of the CTA's Q bases lives in shared
-// memory (t-major, gs[t*Q + base]); T = Q*G threads, G = threads per base, each thread
-// evaluating RPT = 8/G rates of every 8-rate block.  Base b (0 <= b < Q) is side b/(Q/2),
-// k2 = b % (Q/2).
+// memory, t-major with the bases in adjacent pairs interleaved by component: float4
+// gs4[t*(Q/2) + b/2] = {Re F[b0], Re F[b1], Im F[b0], Im F[b1]} for b0 = b & ~1, b1 = b0 + 1,
+// so one 16-byte load gives the packed-FP32 operands (Re, Re) and (Im, Im) of a base pair.
+// T = Q*G threads, G = threads per base pair and rate half; each thread evaluates RT = 4/G
+// rates of every 8-rate block for its two bases, lanes = bases.  Base b (0 <= b < Q) is side
+// b/(Q/2), k2 = b % (Q/2) (a pair never straddles the sides: Q/2 is even).
 // ------------------------------------------------------------------------------------
 template <int Q>
 struct CztSmemShape {
   static constexpr int G = Q >= 512 ? 1 : 2;
   static constexpr int T = Q * G;
-  static constexpr int RPT = kRatesPerBlock / G;
+  static constexpr int RT = 4 / G;
+  // gs starts on a 16-byte boundary (an even float2 offset)
+  static constexpr int GS_OFF = (kRatesPerBlock * b_stride<Q>() + tw_size(Q) + 2 * Q + 1) & ~1;
   template <int NT>
   static constexpr size_t smem() {
-    return sizeof(float2) * (kRatesPerBlock * b_stride<Q>() + tw_size(Q) + 2 * Q + NT * Q + NT);
+    return sizeof(float2) * (GS_OFF + NT * Q + NT);
   }
 };
+
+// F[b, t] in the base-pair interleaved layout of gs (see CztSmemShape).
+__device__ __forceinline__ void gs_put(float2* gs, int Q, int t, int b, float2 v) {
+  float* f = reinterpret_cast<float*>(gs) + ((t * (Q / 2) + (b >> 1)) << 2) + (b & 1);
+  f[0] = v.x;
+  f[2] = v.y;
+}
+__device__ __forceinline__ float2 gs_get(const float2* gs, int Q, int t, int b) {
+  const float* f = reinterpret_cast<const float*>(gs) + ((t * (Q / 2) + (b >> 1)) << 2) + (b & 1);
+  return make_float2(f[0], f[2]);
+}
 
 template <int Q, int NT>
 __device__ __forceinline__ void czt_forward_smem(const CztArgs& a, int c, const int* k1s,
@@ -594,8 +610,8 @@ __device__ __forceinline__ void czt_forward_smem(const CztArgs& a, int c, const 
       const float2 zm = cconj(buf[(2 * u + ms) * SS + pidx(mk2)]);
       const float2 sm_ = cadd(zk, zm), d = csub(zk, zm);
       const int t0 = 2 * (p0 + u);
-      gs[t0 * Q + b] = make_float2(0.5f * sm_.x, 0.5f * sm_.y);
-      if (t0 + 1 < NT) gs[(t0 + 1) * Q + b] = make_float2(0.5f * d.y, -0.5f * d.x);
+      gs_put(gs, Q, t0, b, make_float2(0.5f * sm_.x, 0.5f * sm_.y));
+      if (t0 + 1 < NT) gs_put(gs, Q, t0 + 1, b, make_float2(0.5f * d.y, -0.5f * d.x));
     }
     if (c == 0 && tid == 0) {
       for (int u = 0; u < PC && p0 + u < a.NP; ++u) {
@@ -612,13 +628,13 @@ __device__ __forceinline__ void czt_forward_smem(const CztArgs& a, int c, const 
 template <int Q, int NT>
 __global__ void __launch_bounds__(CztSmemShape<Q>::T, 1) zdtf_czt_smem_kernel(CztArgs a) {
   using SH = CztSmemShape<Q>;
-  constexpr int T = SH::T, RPT = SH::RPT;
+  constexpr int T = SH::T, RT = SH::RT;
   constexpr int SS = b_stride<Q>();
   extern __shared__ float2 sm[];
   float2* buf = sm;
   float2* twt = buf + kRatesPerBlock * SS;
   float2* twr = twt + tw_size(Q);
-  float2* gs = twr + 2 * Q;
+  float2* gs = sm + SH::GS_OFF;
   float2* gnyq = gs + NT * Q;
   const int tid = threadIdx.x;
   const int c = blockIdx.x;
@@ -632,72 +648,102 @@ __global__ void __launch_bounds__(CztSmemShape<Q>::T, 1) zdtf_czt_smem_kernel(Cz
   }
   czt_forward_smem<Q, NT>(a, c, k1s, buf, twt, gs, gnyq);
 
-  const int b = tid % Q, g = tid / Q;
-  const int side = b / (Q / 2), k2 = b - side * (Q / 2);
-  int ms, mk2;
-  mirror_of(c, side, k2, Q, &ms, &mk2);
-  const bool dc = (c == 0 && side == 0 && k2 == 0);
+  // thread -> (base pair bp, rate group rg): bases b0 = 2 bp and b0 + 1 (the two lanes of
+  // every packed operation), rates rg*RT .. rg*RT + RT - 1 of each 8-rate block
+  const int bp = tid % (Q / 2), rg = tid / (Q / 2);
+  const int b0 = 2 * bp;
+  const int side = b0 / (Q / 2), k20 = b0 - side * (Q / 2);
+  int ms[2], mk2[2];
+  mirror_of(c, side, k20, Q, &ms[0], &mk2[0]);
+  mirror_of(c, side, k20 + 1, Q, &ms[1], &mk2[1]);
+  const bool dc = (c == 0 && side == 0 && k20 == 0);  // lane 0 is the DC bin
   const unsigned long long mask = a.ph.mask;
-  const unsigned long long k = (unsigned long long)k1s[side] + (unsigned long long)P * k2;
-  const unsigned long long alpha = (k * a.ph.R0) & mask, beta = (k * a.ph.Rd) & mask;
-  float2 pw[RPT];
+  unsigned long long alpha[2], beta[2];
+  float2 pwx[RT], pwy[RT];  // pw[i] = exact w(k_lane, i*dr), lanes = the two bases
+  float2 win;
 #pragma unroll
-  for (int i = 0; i < RPT; ++i) pw[i] = cis_phase(((unsigned long long)i * beta) & mask, a.ph);
-  const float win = window_value(a, (long long)k);
+  for (int h = 0; h < 2; ++h) {
+    const unsigned long long k = (unsigned long long)k1s[side] + (unsigned long long)P * (k20 + h);
+    alpha[h] = (k * a.ph.R0) & mask;
+    beta[h] = (k * a.ph.Rd) & mask;
+#pragma unroll
+    for (int i = 0; i < RT; ++i) {
+      const float2 p = cis_phase(((unsigned long long)i * beta[h]) & mask, a.ph);
+      if (h == 0) { pwx[i].x = p.x; pwy[i].x = p.y; } else { pwx[i].y = p.x; pwy[i].y = p.y; }
+    }
+    const float wv = window_value(a, (long long)k);
+    if (h == 0) win.x = wv; else win.y = wv;
+  }
   const unsigned long long kny = (unsigned long long)(a.N / 2);
   const unsigned long long alpha_n = (kny * a.ph.R0) & mask, beta_n = (kny * a.ph.Rd) & mask;
   const int Nt = a.Nt;
+  const float4* gs4 = reinterpret_cast<const float4*>(gs);
 
   const int q_begin = blockIdx.y * a.pairs_per_group;
   const int q_end = min(a.npairs, q_begin + a.pairs_per_group);
   for (int q0 = q_begin; q0 < q_end; q0 += kRatesPerBlock / 2) {
-    const int j0 = 2 * q0 + g * RPT;  // this thread's first rate of the block
+    const int j0 = 2 * q0 + rg * RT;  // this thread's first rate of the block
     const long long jb = a.blk_base ? (long long)__ldg(a.blk_base + (q0 >> 2)) : (long long)(2 * q0);
-    const float2 w0 = cis_phase((alpha + (unsigned long long)(jb + g * RPT) * beta) & mask, a.ph);
-    // Horner's rule for the RPT rates, two rates per packed-FP32 lane pair
-    constexpr int RP = RPT / 2;
-    float2 Wx[RP], Wy[RP], NWy[RP], Sx[RP], Sy[RP];
+    // w(k_lane, first rate) exact; the thread's other rates = that * pw[i] (exact pw)
+    float2 W0x, W0y;
     {
-      const float2 gl = gs[(Nt - 1) * Q + b];
+      const unsigned long long jj = (unsigned long long)(jb + rg * RT);
+      const float2 w0 = cis_phase((alpha[0] + jj * beta[0]) & mask, a.ph);
+      const float2 w1 = cis_phase((alpha[1] + jj * beta[1]) & mask, a.ph);
+      W0x = make_float2(w0.x, w1.x);
+      W0y = make_float2(w0.y, w1.y);
+    }
+    float2 Wx[RT], Wy[RT], NWy[RT], Sx[RT], Sy[RT];
+    {
+      const float2 NW0y = pk_neg(W0y);
+      const float4 gl = gs4[(Nt - 1) * (Q / 2) + bp];
 #pragma unroll
-      for (int u = 0; u < RP; ++u) {
-        const float2 wa = cmul(w0, pw[2 * u]), wc = cmul(w0, pw[2 * u + 1]);
-        Wx[u] = make_float2(wa.x, wc.x);
-        Wy[u] = make_float2(wa.y, wc.y);
-        NWy[u] = pk_neg(Wy[u]);
-        Sx[u] = make_float2(gl.x, gl.x);
-        Sy[u] = make_float2(gl.y, gl.y);
+      for (int r = 0; r < RT; ++r) {
+        if (r == 0) {
+          Wx[r] = W0x;
+          Wy[r] = W0y;
+        } else {
+          Wx[r] = pk_fma(W0x, pwx[r], pk_mul(NW0y, pwy[r]));
+          Wy[r] = pk_fma(W0x, pwy[r], pk_mul(W0y, pwx[r]));
+        }
+        NWy[r] = pk_neg(Wy[r]);
+        Sx[r] = make_float2(gl.x, gl.y);
+        Sy[r] = make_float2(gl.z, gl.w);
       }
     }
+    // Horner's rule over t for the thread's RT rates, both bases in the packed lanes
+#pragma unroll 4
     for (int t = Nt - 2; t >= 0; --t) {
-      const float2 gt = gs[t * Q + b];
-      const float2 gx = make_float2(gt.x, gt.x), gy = make_float2(gt.y, gt.y);
+      const float4 gt = gs4[t * (Q / 2) + bp];
+      const float2 gx = make_float2(gt.x, gt.y), gy = make_float2(gt.z, gt.w);
 #pragma unroll
-      for (int u = 0; u < RP; ++u) {
-        const float2 tx = pk_fma(Sx[u], Wx[u], pk_fma(Sy[u], NWy[u], gx));
-        const float2 ty = pk_fma(Sx[u], Wy[u], pk_fma(Sy[u], Wx[u], gy));
-        Sx[u] = tx;
-        Sy[u] = ty;
+      for (int r = 0; r < RT; ++r) {
+        const float2 tx = pk_fma(Sx[r], Wx[r], pk_fma(Sy[r], NWy[r], gx));
+        const float2 ty = pk_fma(Sx[r], Wy[r], pk_fma(Sy[r], Wx[r], gy));
+        Sx[r] = tx;
+        Sy[r] = ty;
       }
-    }
-    float2 S[RPT];
-#pragma unroll
-    for (int u = 0; u < RP; ++u) {
-      S[2 * u] = make_float2(Sx[u].x, Sy[u].x);
-      S[2 * u + 1] = make_float2(Sx[u].y, Sy[u].y);
     }
     __syncthreads();  // buf is free
 #pragma unroll
-    for (int u2 = 0; u2 < RPT / 2; ++u2) {
-      const int u = g * (RPT / 2) + u2;
-      float2 sa = S[2 * u2], sb = S[2 * u2 + 1];
-      sa = (j0 + 2 * u2 < a.Nr) ? cscale(sa, win) : make_float2(0.f, 0.f);
-      sb = (j0 + 2 * u2 + 1 < a.Nr) ? cscale(sb, win) : make_float2(0.f, 0.f);
-      if (dc) {
-        buf[(2 * u) * SS + pidx(0)] = make_float2(sa.x, sb.x);
-      } else {
-        buf[(2 * u + side) * SS + pidx(k2)] = make_float2(sa.x - sb.y, sa.y + sb.x);
-        buf[(2 * u + ms) * SS + pidx(mk2)] = make_float2(sa.x + sb.y, sb.x - sa.y);
+    for (int up = 0; up < RT / 2; ++up) {
+      const int u = rg * (RT / 2) + up;  // rate pair within the block
+      const bool ok_a = j0 + 2 * up < a.Nr, ok_b = j0 + 2 * up + 1 < a.Nr;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const float wh = h ? win.y : win.x;
+        const float2 sa = ok_a ? cscale(make_float2(h ? Sx[2 * up].y : Sx[2 * up].x,
+                                                    h ? Sy[2 * up].y : Sy[2 * up].x), wh)
+                               : make_float2(0.f, 0.f);
+        const float2 sb = ok_b ? cscale(make_float2(h ? Sx[2 * up + 1].y : Sx[2 * up + 1].x,
+                                                    h ? Sy[2 * up + 1].y : Sy[2 * up + 1].x), wh)
+                               : make_float2(0.f, 0.f);
+        if (dc && h == 0) {
+          buf[(2 * u) * SS + pidx(0)] = make_float2(sa.x, sb.x);
+        } else {
+          buf[(2 * u + side) * SS + pidx(k20 + h)] = make_float2(sa.x - sb.y, sa.y + sb.x);
+          buf[(2 * u + ms[h]) * SS + pidx(mk2[h])] = make_float2(sa.x + sb.y, sb.x - sa.y);
+        }
       }
     }
     if (c == 0 && tid == 0) {
@@ -736,7 +782,7 @@ __global__ void __launch_bounds__(CztSmemShape<Q>::T, 1) zdtf_a2f_smem_kernel(Cz
   float2* buf = sm;
   float2* twt = buf + kRatesPerBlock * SS;
   float2* twr = twt + tw_size(Q);
-  float2* gs = twr + 2 * Q;
+  float2* gs = sm + SH::GS_OFF;
   float2* gnyq = gs + NT * Q;
   const int tid = threadIdx.x;
   const int c = blockIdx.x;
@@ -749,7 +795,7 @@ __global__ void __launch_bounds__(CztSmemShape<Q>::T, 1) zdtf_a2f_smem_kernel(Cz
     const int t = e / Q, b = e - t * Q;
     const int side = b / (Q / 2), k2 = b - side * (Q / 2);
     if (FDR_DBG_OK((long long)k1s[side] + (long long)P * k2 + t * K < K * a.Nt))
-      a.F[(long long)k1s[side] + (long long)P * k2 + t * K] = gs[t * Q + b];
+      a.F[(long long)k1s[side] + (long long)P * k2 + t * K] = gs_get(gs, Q, t, b);
   }
   if (c == 0 && tid == 0)
     for (int t = 0; t < a.Nt; ++t) a.F[a.N / 2 + t * K] = gnyq[t];
