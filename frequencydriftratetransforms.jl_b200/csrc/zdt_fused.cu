@@ -577,27 +577,31 @@ __device__ __forceinline__ void czt_forward_smem(const CztArgs& a, int c, const 
   for (int i = tid; i < NT * Q; i += T) gs[i] = make_float2(0.f, 0.f);
   if (c == 0 && tid == 0)
     for (int t = 0; t < NT; ++t) gnyq[t] = make_float2(0.f, 0.f);
+  // A rows of chunk p0 (PC t pairs x 2 sides) into registers; the next chunk's loads are
+  // issued before the current chunk's FFT, so their latency overlaps it
+  constexpr int NL = 2 * PC * Q / T;
+  float2 v[NL];
+  auto load_chunk = [&](int p0) {
+#pragma unroll
+    for (int i = 0; i < NL; ++i) {
+      const int e = tid + i * T;
+      const int seq = e / Q, na = e - seq * Q;
+      const int pp = p0 + (seq >> 1), side = seq & 1;
+      v[i] = (pp < a.NP && FDR_DBG_OK(((long long)pp * a.P + k1s[side]) * Q + na < (long long)a.NP * a.P * Q))
+                 ? __ldcs(a.A + ((long long)pp * a.P + k1s[side]) * Q + na)
+                 : make_float2(0.f, 0.f);
+    }
+  };
+  load_chunk(0);
   for (int p0 = 0; p0 < a.NP; p0 += PC) {
     __syncthreads();
-    {
-      constexpr int NL = 2 * PC * Q / T;
-      float2 v[NL];
 #pragma unroll
-      for (int i = 0; i < NL; ++i) {
-        const int e = tid + i * T;
-        const int seq = e / Q, na = e - seq * Q;
-        const int pp = p0 + (seq >> 1), side = seq & 1;
-        v[i] = (pp < a.NP && FDR_DBG_OK(((long long)pp * a.P + k1s[side]) * Q + na < (long long)a.NP * a.P * Q))
-                   ? __ldcs(a.A + ((long long)pp * a.P + k1s[side]) * Q + na)
-                           : make_float2(0.f, 0.f);
-      }
-#pragma unroll
-      for (int i = 0; i < NL; ++i) {
-        const int e = tid + i * T;
-        const int seq = e / Q, na = e - seq * Q;
-        buf[seq * SS + pidx(na)] = v[i];
-      }
+    for (int i = 0; i < NL; ++i) {
+      const int e = tid + i * T;
+      const int seq = e / Q, na = e - seq * Q;
+      buf[seq * SS + pidx(na)] = v[i];
     }
+    if (p0 + PC < a.NP) load_chunk(p0 + PC);
     __syncthreads();
     smem_fft<Q, 2 * PC, SS, T, -1>(buf, twt);
     for (int e = tid; e < PC * Q; e += T) {
