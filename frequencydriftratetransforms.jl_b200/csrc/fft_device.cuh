@@ -350,6 +350,76 @@ __device__ __forceinline__ void smem_fft_emit(float2* buf, const float2* twt, Em
   stockham_passes_emit<LEN, NSEQ, SSTRIDE, T, SIGN, 1>(buf, twt, emit);
 }
 
+// ------------------------------------------------------------------------------------
+// FFTs by a group of whole warps of a block (warp-specialised kernels): the group's T
+// threads, numbered ltid = 0..T-1, synchronise on hardware named barrier BAR (bar.sync with
+// a thread count: no other warp of the block takes part).
+// ------------------------------------------------------------------------------------
+template <int ID, int NTHR>
+__device__ __forceinline__ void named_sync() {
+  asm volatile("bar.sync %0, %1;" ::"n"(ID), "n"(NTHR) : "memory");
+}
+template <int ID, int NTHR>
+__device__ __forceinline__ void named_arrive() {
+  asm volatile("bar.arrive %0, %1;" ::"n"(ID), "n"(NTHR) : "memory");
+}
+
+// In-place Stockham FFT of NSEQ sequences (layout as smem_fft) by a group of T threads whose
+// last pass hands each output to emit(seq, i, value); the inputs must be visible to the group
+// when it is called.  Every pass but the last reads its butterflies into registers, waits for
+// the group, writes, and waits again; the last pass only reads, so the buffer may be reused
+// once every thread of the group has returned.
+template <int LEN, int NSEQ, int SSTRIDE, int T, int SIGN, int BAR, int NS, class Emit>
+__device__ __forceinline__ void group_fft_emit(float2* buf, const float2* twt, int ltid, Emit emit) {
+  constexpr int R = plan_radix(LEN / NS);
+  constexpr int NBF = LEN / R;
+  constexpr int NB = NBF * NSEQ;
+  constexpr int PER = (NB + T - 1) / T;
+  const float2* tw = twt + tw_offset(LEN, NS);
+  float2 v[PER][R];
+#pragma unroll
+  for (int i = 0; i < PER; ++i) {
+    const int j = ltid + i * T;
+    if (NB % T == 0 || j < NB) {
+      const int seq = j / NBF, jj = j - seq * NBF;
+      const float2* a = buf + seq * SSTRIDE;
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[i][r] = a[pidx(jj + r * NBF)];
+    }
+  }
+  if constexpr (NS * R < LEN) named_sync<BAR, T>();  // every input read before any write
+#pragma unroll
+  for (int i = 0; i < PER; ++i) {
+    const int j = ltid + i * T;
+    if (NB % T == 0 || j < NB) {
+      const int seq = j / NBF, jj = j - seq * NBF;
+      const int k = jj % NS;
+      if (NS > 1) {
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          float2 w = tw[(r - 1) * NS + k];
+          if (SIGN > 0) w.y = -w.y;
+          v[i][r] = cmul(v[i][r], w);
+        }
+      }
+      Dft<R>::run(v[i], SIGN);
+      const int base = (jj / NS) * NS * R + k;
+      if constexpr (NS * R < LEN) {
+        float2* b = buf + seq * SSTRIDE;
+#pragma unroll
+        for (int r = 0; r < R; ++r) b[pidx(base + r * NS)] = v[i][r];
+      } else {
+#pragma unroll
+        for (int r = 0; r < R; ++r) emit(seq, base + r * NS, v[i][r]);
+      }
+    }
+  }
+  if constexpr (NS * R < LEN) {
+    named_sync<BAR, T>();  // the pass's outputs are visible to the group
+    group_fft_emit<LEN, NSEQ, SSTRIDE, T, SIGN, BAR, NS * R>(buf, twt, ltid, emit);
+  }
+}
+
 template <int LEN, int NSEQ, int SSTRIDE, int T, int SIGN, int NS>
 __device__ __forceinline__ void stockham_passes(float2* buf, const float2* twt) {
   if constexpr (NS < LEN) {
