@@ -444,7 +444,14 @@ def main():
                     help="skip the Taylor-tree vs intfdr leg")
     ap.add_argument("--no-fp32-peak", action="store_true",
                     help="skip the SGEMM measurement of the FP32 peak (compute.frac)")
+    ap.add_argument("--nt", type=int, default=16,
+                    help="time steps of the synthetic spectrograms (16: the headline "
+                         "configuration; 32 or 64 profile the shared-memory czt kernels)")
     args = ap.parse_args()
+    if args.nt != 16:
+        global NT, WORKLOAD
+        NT = args.nt
+        WORKLOAD = WORKLOAD.replace("Nt=16", f"Nt={NT}")
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -625,8 +632,8 @@ def main():
             "config": {"workload": WORKLOAD, "Nf": NF, "Nt": NT, "Nr": NR, "Nl": ws.Nl,
                        "path": "staged" if (args.staged or not ws.fused) else "fused",
                        "parallelism": f"replicas x{world} (independent channels)",
-                       "l2": "4 rotating 64 MiB spectrograms (256 MiB > L2) and a 541 MB "
-                             "FDR output per step"},
+                       "l2": f"4 rotating {4 * NF * NT >> 20} MiB spectrograms "
+                             f"({16 * NF * NT >> 20} MiB > L2) and a 541 MB FDR output per step"},
             "e2e": {"value": e2e_value, "unit": "cells/s",
                     "h2d_bytes_per_step": 4 * NF * NT,
                     "d2h_bytes_per_step": int(16 * nh_total / max(1, e2e_steps)) + 8,
@@ -638,8 +645,9 @@ def main():
                             "zdtfdr! with fused findprotohits(snr=10) -> hits to host"},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": NCU_TRAFFIC["bytes_per_call"],
-                         "traffic_capture": NCU_TRAFFIC["capture"],
+                         "frac": achieved / peak,
+                         "traffic": NCU_TRAFFIC["bytes_per_call"] if NT == 16 else None,
+                         "traffic_capture": NCU_TRAFFIC["capture"] if NT == 16 else None,
                          "kernel": "whole ZDT call (all launches of one zdtfdr!)",
                          "algorithmic_bytes": algorithmic_bytes(), "peak_source": peak_src},
             "compute": {"flop_nominal": flops, "achieved_tflops": flops / (ms_step * 1e-3) / 1e12,
