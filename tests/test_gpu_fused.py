@@ -79,6 +79,27 @@ def test_fused_windows_and_batches(fdr, oracle):
         assert oracle.rel_linf(d.cpu().numpy(), truth) < 1e-5
 
 
+@pytest.mark.parametrize("Nf,Nt,Nr", [(2 ** 16, 32, 41), (2 ** 17, 64, 65), (2 ** 15, 24, 9), (2 ** 19, 20, 17)])
+def test_fused_windows_and_batches_shared_memory_f(fdr, oracle, Nf, Nt, Nr):
+    """16 < Nt <= 64 with 256 or 512 bins per czt CTA (the warp-specialised czt kernel):
+    Hamming and custom windows and an r0 list against the staged kernels and FP64."""
+    P, Q = fdr.fused_split(Nf, Nt, Nr)
+    assert Q in (256, 512)
+    spec = _spec(oracle, Nf, Nt, seed=3 * Nf + Nt)
+    ws = fdr.ZDTWorkspace(spec, -2.0, 1 / 16, Nr)
+    st = fdr.ZDTWorkspace(spec, -2.0, 1 / 16, Nr, staged_only=True)
+    for w in ("hamming", lambda n, N: 1.0 - n / N):
+        a = fdr.zdtfdr(ws, w=w).cpu().numpy()
+        b = fdr.zdtfdr(st, w=w).cpu().numpy()
+        assert oracle.rel_linf(a, b) < 2e-5
+    dests = [fdr.fortran_empty(Nf, Nr) for _ in range(2)]
+    fdr.zdtfdr_(dests, ws, r0=[-3.0, 0.5])
+    for d, r0 in zip(dests, [-3.0, 0.5]):
+        cols = [0, Nr // 2, Nr - 1]
+        truth = oracle.fdr_truth(spec, [r0 + j / 16 for j in cols])
+        assert oracle.rel_linf(d.cpu().numpy()[:, cols], truth) < 1e-5
+
+
 def test_fused_input_then_staged_stages(fdr, oracle):
     """input! through the fused path, then the staged stages read F (rebuilt from the fused
     input stage) -- equal to a staged-only workspace's F."""
