@@ -1,7 +1,7 @@
 """Batches of coarse channels in one CUDA-graph launch (fdr_batch_* in the C ABI).
 
 The reference computes one zdtfdr! per spectrogram and leaves the loop over coarse channels
-to the pipeline (README.md:57-71).  ZDTBatch plans that loop once: channels of any shapes
+to the pipeline (the reference's README.md:57-71).  ZDTBatch plans that loop once: channels of any shapes
 (Nf, Nt, rate set) share fused plans by shape, run over several streams, are tuned by the
 library's autotuner and replay as a single CUDA graph.
 """

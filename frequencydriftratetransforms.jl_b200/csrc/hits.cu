@@ -2,7 +2,7 @@
 //
 // findprotohits (fdrutils.jl:148-169) returns every FDR cell above threshold; one drifting
 // signal is seen at several neighbouring (frequency, drift rate) cells, and the step after
-// it, "detection of unique signals ... within the proto-hits" (README.md:57-66), lives
+// it, "detection of unique signals ... within the proto-hits" (the reference's README.md:57-66), lives
 // outside the reference (DopplerDriftSearchTools.jl).  This is that step on the device:
 // the connected components of the proto-hits under a (di, dj) neighbourhood (|Δi| <= di
 // channels, |Δj| <= dj drift-rate columns, no wrap-around), with per-cluster counts,

@@ -2,7 +2,7 @@
 //
 // The reference computes integer-shift FDRs by brute force (intfdr, intfdr.jl:34-45) and
 // notes that "the Taylor Tree algorithm" would remove the redundant additions but is not
-// included (README.md:88-92).  This is that algorithm for Nt = 2^m time steps: FDR column d
+// included (the reference's README.md:88-92).  This is that algorithm for Nt = 2^m time steps: FDR column d
 // (total drift d channels over the Nt-1 step intervals, rate d/(Nt-1) channels per step,
 // |d| <= Nt-1) is the sum of the spectrogram along a tree path built recursively: a path of
 // drift d over 2L steps is the path of drift floor(d/2) over the first L steps followed by

@@ -1,6 +1,6 @@
 // Batched ZDT over many coarse channels of uneven shape (Nf, Nt, rates) in one CUDA-graph
 // launch.  The reference processes one spectrogram per zdtfdr! call; a pipeline such as
-// DopplerDriftSearchPipeline.jl loops over coarse channels (README.md:57-71).  Here the
+// DopplerDriftSearchPipeline.jl loops over coarse channels (the reference's README.md:57-71).  Here the
 // loop is captured once: channels are spread over `slots` streams forked from the caller's
 // stream, each slot owning the fused path's intermediates (A, W) sized for the largest
 // channel, channels of equal (Nf, Nt, Nr) share one FusedPlan (twiddle tables), and the

@@ -2,7 +2,7 @@
 
 The reference's own data path reads a rawspec product with HDF5 (test/heavytests.jl:11-14:
 ``h5["data"][freq_range, 1, :]``, a (channel, IF, time) view of a (time, IF, channel)
-dataset) and leaves the search pipeline to DopplerDriftSearchPipeline.jl (README.md:68-71).
+dataset) and leaves the search pipeline to DopplerDriftSearchPipeline.jl (the reference's README.md:68-71).
 HDF5 with the bitshuffle filter needs libhdf5 and its plugin, which this environment does
 not have; rawspec writes the same spectra as SIGPROC filterbank files, which are read here:
 a keyword header (HEADER_START ... HEADER_END) followed by time-major samples, each

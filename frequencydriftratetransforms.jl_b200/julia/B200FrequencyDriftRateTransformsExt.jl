@@ -328,7 +328,7 @@ function intfdr!(fdr::CuMatrix{Float32}, spectrogram::CuMatrix{Float32}, rates)
     return fdr
 end
 
-# The Taylor-tree integer FDR (README.md:88-92; no counterpart in the reference code):
+# The Taylor-tree integer FDR (the reference's README.md:88-92; no counterpart in the reference code):
 # columns d = dmin..dmax of fdr, drift d channels over Nt-1 steps.
 function taylorfdr!(fdr::CuMatrix{Float32}, spectrogram::CuMatrix{Float32}, drange::UnitRange{<:Integer})
     Nf, Nt = size(spectrogram)

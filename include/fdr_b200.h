@@ -217,7 +217,7 @@ int fdr_zdt_stage_times(fdr_zdt* ws, float* times_ms, int max_stages, int* nstag
 
 /* ---------------------------------------------------------------------------------- */
 /* Batches of coarse channels (no single reference function: the reference runs one      */
-/* zdtfdr! per spectrogram; pipelines loop over coarse channels, README.md:57-71)          */
+/* zdtfdr! per spectrogram; pipelines loop over coarse channels, its README.md:57-71)     */
 /* ---------------------------------------------------------------------------------- */
 typedef struct fdr_batch fdr_batch;
 typedef struct fdr_batch_channel {
@@ -308,8 +308,8 @@ int fdr_intfdr(const float* spec, int64_t Nf, int64_t Nt, const double* rates, i
    (shift of rate j at time t at shifts[j*Nt + t]). */
 int fdr_intfdr_shifts(const float* spec, int64_t Nf, int64_t Nt, const int64_t* shifts,
                       int64_t Nr, float* fdr, fdr_stream_t stream);
-/* Taylor-tree integer FDR (the faster intfdr variant README.md:88-92 mentions; no
-   counterpart in the reference code).  Nt a power of two in [2, 64]; column d - dmin of
+/* Taylor-tree integer FDR (the faster intfdr variant the reference's README.md:88-92
+   mentions; no counterpart in the reference code).  Nt a power of two in [2, 64]; column d - dmin of
    fdr (device, Nf x (dmax-dmin+1) column-major) for each integer total drift d in
    [dmin, dmax] (|d| <= Nt-1, rate d/(Nt-1) channels per step) sums
    spec[(n + p_d(t)) mod Nf, t] along the tree path p_d: p_d = 0 for Nt = 1, and over 2L
@@ -396,7 +396,7 @@ int fdr_findprotohits(const float* const* fdrs, int64_t nb, int64_t Nf, int64_t 
 
 /* ---------------------------------------------------------------------------------- */
 /* Proto-hits -> hits.  No counterpart in the reference: it is the step after           */
-/* findprotohits that README.md:57-66 places in DopplerDriftSearchTools.jl.             */
+/* findprotohits that its README.md:57-66 places in DopplerDriftSearchTools.jl.           */
 /* ---------------------------------------------------------------------------------- */
 typedef struct fdr_hit_cluster {
   int64_t peak_i, peak_j; /* zero-based cell of the largest FDR value (first in column-major

@@ -810,7 +810,7 @@ def cluster_protohits(hits, Nf, di=1, dj=1, fdr=None):
 
 
 # ----------------------------------------------------------------------------------------
-# Taylor tree (the faster integer FDR that README.md:88-92 mentions)
+# Taylor tree (the faster integer FDR that the reference's README.md:88-92 mentions)
 # ----------------------------------------------------------------------------------------
 
 def taylor_tree(spec, dmin, dmax):

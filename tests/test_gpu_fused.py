@@ -1,7 +1,7 @@
-"""GPU parity tests of the fused ZDT kernels (power-of-two Nf, Nt <= 16) against the staged
+"""GPU parity tests of the fused ZDT kernels (power-of-two Nf, Nt <= 64) against the staged
 kernels and the CPU oracle.
 
-Tolerances (relative L-infinity): 1e-4 vs FP64 (the fused path reduces
+Tolerances (relative L-infinity): 1e-4 vs FP64 (the accuracy bound of the FDR; the fused path reduces
 chirp phases exactly and is typically ~1e-6); 2e-5 vs the staged kernels and the FP32
 mirror, which carry the reference's Float32 phase-argument rounding (~5e-6 at Nf=2^20).
 """

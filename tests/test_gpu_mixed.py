@@ -1,6 +1,6 @@
 """Mixed-precision ZDT (FDR_ZDT_MIXED_PRECISION): the output pass's DFTs as split-bfloat16
 tensor-core contractions.  Tolerances (relative L-infinity of the FDR's peak): 1e-4 against
-FP64 (measured ~2e-6) and 2e-5 against the FP32 plain form."""
+FP64 (the accuracy bound of the FDR; measured ~2e-6) and 2e-5 against the FP32 plain form."""
 import numpy as np
 import pytest
 

@@ -1,7 +1,7 @@
 """GPU parity tests of the ZDT path (zdtfdr.jl) through the C ABI against the CPU oracle.
 
 Tolerances (relative L-infinity, max|a-b| / max|b|):
-  * vs the FP64 oracle: 1e-4; the library is typically ~1e-6 at
+  * vs the FP64 oracle: 1e-4 (the accuracy bound of the FDR); the library is typically ~1e-6 at
     Nf <= 65536 and ~5e-6 at Nf = 2^20 with the reference's Float32 phase arguments.
   * vs the FP32 mirror of the reference: 2e-5 (both carry float32 rounding of their own
     FFTs; the phase arguments are the same Float32 values).
