@@ -517,13 +517,16 @@ __global__ void __launch_bounds__(Q / 2, (Q <= 512 ? 2 : 1)) zdtf_czt_kernel(Czt
       }
     }
     __syncthreads();
-    // inverse DFT_Q; its last pass writes W (with the inter-pass twiddle and 1/Nf) directly
-    float2* const W = a.W;
+    // inverse DFT_Q; its last pass writes W (with the inter-pass twiddle and 1/Nf) directly.
+    // Row (q0 + p, k1) of W starts at Wq + (p*P + k1)*Q: a 32-bit offset (p < 4; the fused
+    // path has P*Q = Nf <= 2^22).
+    float2* const Wq = a.W + (long long)q0 * P * Q;
     const int k1a = k1s[0], k1b = k1s[1];
     stockham_passes_emit_pp<Q, kRatesPerBlock, SS, T, +1, 1>(hb, ob, twt, [&](int seq, int na, float2 v) {
-      const int q = q0 + (seq >> 1), side = seq & 1;
-      if (q < q_end && FDR_DBG_OK(((long long)q * P + (side ? k1b : k1a)) * Q + na < (long long)a.npairs * P * Q))
-        W[((long long)q * P + (side ? k1b : k1a)) * Q + na] = cmul(v, twr[side * Q + na]);
+      const int p = seq >> 1, side = seq & 1;
+      const unsigned off = (unsigned)((p * P + (side ? k1b : k1a)) * Q + na);
+      if (q0 + p < q_end && FDR_DBG_OK((long long)(q0 + p) * P * Q + off < (long long)a.npairs * P * Q))
+        Wq[off] = cmul(v, twr[side * Q + na]);
     });
     if (kFlip) {
       float2* t = hb;
@@ -974,16 +977,17 @@ __global__ void __launch_bounds__(CztWsShape<Q>::T, 1) zdtf_czt_ws_kernel(CztArg
   } else {
     // ---------------- FFT threads ----------------
     const int ltid = tid - H;
-    float2* const W = a.W;
     const int k1a = k1s[0], k1b = k1s[1];
     for (int ib = 0; ib < nblk; ++ib) {
       const int q0 = q_begin + ib * (kRatesPerBlock / 2);
       float2* const hb = (ib & 1) ? buf1 : buf0;
+      float2* const Wq = a.W + (long long)q0 * P * Q;  // 32-bit offsets below (Nf <= 2^22)
       if (ib & 1) named_sync<kBarFull + 1, T>(); else named_sync<kBarFull, T>();
       group_fft_emit<Q, kRatesPerBlock, SS, I, +1, kBarFft, 1>(hb, twt, ltid, [&](int seq, int na, float2 v) {
-        const int q = q0 + (seq >> 1), sd = seq & 1;
-        if (q < q_end && FDR_DBG_OK(((long long)q * P + (sd ? k1b : k1a)) * Q + na < (long long)a.npairs * P * Q))
-          W[((long long)q * P + (sd ? k1b : k1a)) * Q + na] = cmul(v, twr[sd * Q + na]);
+        const int p = seq >> 1, sd = seq & 1;
+        const unsigned off = (unsigned)((p * P + (sd ? k1b : k1a)) * Q + na);
+        if (q0 + p < q_end && FDR_DBG_OK((long long)(q0 + p) * P * Q + off < (long long)a.npairs * P * Q))
+          Wq[off] = cmul(v, twr[sd * Q + na]);
       });
       if (ib + 2 < nblk) {
         if (ib & 1) named_arrive<kBarEmpty + 1, T>(); else named_arrive<kBarEmpty, T>();
