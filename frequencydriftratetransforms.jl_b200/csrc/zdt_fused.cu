@@ -25,7 +25,9 @@
 // hence dyadic, so k*r_j/Nf is an exact fraction m / 2^bits with m computed in 64-bit
 // integer arithmetic modulo 2^bits; only the final conversion to a float in [-1, 1)
 // half-turns rounds.
+#define FDR_TU_ID 1  // index violations of the debug build report this file as unit 1
 #include <cuda.h>  // CUtensorMap (the encode entry point is fetched from the runtime)
+#include <cooperative_groups.h>
 #include <cuda_bf16.h>
 #include <cudaTypedefs.h>
 #include <math.h>
@@ -34,6 +36,8 @@
 #include "fft_device.cuh"
 #include "fft_engine.cuh"
 #include "zdt_ws.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace fdr {
 
@@ -525,7 +529,7 @@ __global__ void __launch_bounds__(Q / 2, (Q <= 512 ? 2 : 1)) zdtf_czt_kernel(Czt
     stockham_passes_emit_pp<Q, kRatesPerBlock, SS, T, +1, 1>(hb, ob, twt, [&](int seq, int na, float2 v) {
       const int p = seq >> 1, side = seq & 1;
       const unsigned off = (unsigned)((p * P + (side ? k1b : k1a)) * Q + na);
-      if (q0 + p < q_end && FDR_DBG_OK((long long)(q0 + p) * P * Q + off < (long long)a.npairs * P * Q))
+      if (q0 + p < q_end && FDR_DBG_OK((long long)q0 * P * Q + off < (long long)a.npairs * P * Q))
         Wq[off] = cmul(v, twr[side * Q + na]);
     });
     if (kFlip) {
@@ -570,15 +574,17 @@ __device__ __forceinline__ float2 gs_get(const float2* gs, int Q, int t, int b) 
 }
 
 // Forward DFT_Q of the CTA's A rows for all t into gs (pair-interleaved F), by all T
-// threads of the block.
-template <int Q, int NT, int T = CztSmemShape<Q>::T>
+// threads of the block.  HALF: keep only the bins of side own_side (Q/2 bins per row of gs;
+// the DFTs of both sides are still computed, the two-for-one unpacking needs both).
+template <int Q, int NT, int T = CztSmemShape<Q>::T, bool HALF = false>
 __device__ __forceinline__ void czt_forward_smem(const CztArgs& a, int c, const int* k1s,
                                                  float2* buf, const float2* twt, float2* gs,
-                                                 float2* gnyq) {
+                                                 float2* gnyq, int own_side = 0) {
   constexpr int SS = b_stride<Q>();
   constexpr int PC = 4;
+  constexpr int QROW = HALF ? Q / 2 : Q;  // bins per row of gs
   const int tid = threadIdx.x;
-  for (int i = tid; i < NT * Q; i += T) gs[i] = make_float2(0.f, 0.f);
+  for (int i = tid; i < NT * QROW; i += T) gs[i] = make_float2(0.f, 0.f);
   if (c == 0 && tid == 0)
     for (int t = 0; t < NT; ++t) gnyq[t] = make_float2(0.f, 0.f);
   // A rows of chunk p0 (PC t pairs x 2 sides) into registers; the next chunk's loads are
@@ -610,8 +616,9 @@ __device__ __forceinline__ void czt_forward_smem(const CztArgs& a, int c, const 
     if (p0 + PC < a.NP) load_chunk(p0 + PC);
     __syncthreads();
     smem_fft<Q, 2 * PC, SS, T, -1>(buf, twt);
-    for (int e = tid; e < PC * Q; e += T) {
-      const int u = e / Q, b = e - u * Q;
+    for (int e = tid; e < PC * QROW; e += T) {
+      const int u = e / QROW;
+      const int b = e - u * QROW + (HALF ? own_side * (Q / 2) : 0);
       if (p0 + u >= a.NP) continue;
       const int side = b / (Q / 2), k2 = b - side * (Q / 2);
       int ms, mk2;
@@ -620,8 +627,9 @@ __device__ __forceinline__ void czt_forward_smem(const CztArgs& a, int c, const 
       const float2 zm = cconj(buf[(2 * u + ms) * SS + pidx(mk2)]);
       const float2 sm_ = cadd(zk, zm), d = csub(zk, zm);
       const int t0 = 2 * (p0 + u);
-      gs_put(gs, Q, t0, b, make_float2(0.5f * sm_.x, 0.5f * sm_.y));
-      if (t0 + 1 < NT) gs_put(gs, Q, t0 + 1, b, make_float2(0.5f * d.y, -0.5f * d.x));
+      const int bg = HALF ? k2 : b;  // bin within gs's row
+      gs_put(gs, QROW, t0, bg, make_float2(0.5f * sm_.x, 0.5f * sm_.y));
+      if (t0 + 1 < NT) gs_put(gs, QROW, t0 + 1, bg, make_float2(0.5f * d.y, -0.5f * d.x));
     }
     if (c == 0 && tid == 0) {
       for (int u = 0; u < PC && p0 + u < a.NP; ++u) {
@@ -986,7 +994,7 @@ __global__ void __launch_bounds__(CztWsShape<Q>::T, 1) zdtf_czt_ws_kernel(CztArg
       group_fft_emit<Q, kRatesPerBlock, SS, I, +1, kBarFft, 1>(hb, twt, ltid, [&](int seq, int na, float2 v) {
         const int p = seq >> 1, sd = seq & 1;
         const unsigned off = (unsigned)((p * P + (sd ? k1b : k1a)) * Q + na);
-        if (q0 + p < q_end && FDR_DBG_OK((long long)(q0 + p) * P * Q + off < (long long)a.npairs * P * Q))
+        if (q0 + p < q_end && FDR_DBG_OK((long long)q0 * P * Q + off < (long long)a.npairs * P * Q))
           Wq[off] = cmul(v, twr[sd * Q + na]);
       });
       if (ib + 2 < nblk) {
@@ -994,6 +1002,269 @@ __global__ void __launch_bounds__(CztWsShape<Q>::T, 1) zdtf_czt_ws_kernel(CztArg
       }
     }
   }
+}
+
+// ------------------------------------------------------------------------------------
+// Kernel B for 32 < Nt <= 64 with 512 bins per residue pair (the split 2048 x 512 at Nf =
+// 2^20 and 4096 x 512 at 2^21, instead of 4096 x 256 / 8192 x 256): F of 64 steps for 512
+// bins (256 KB) does not fit one CTA, so a cluster of two CTAs shares the residue pair.  CTA
+// rank s keeps F of side s (residue k1 or P - k1: 256 bins, 128 KB) and evaluates Horner's
+// rule for them.  Each rate pair of a block has an owner (pairs 0 and 1: rank 0; 2 and 3:
+// rank 1); every CTA writes its sums, at the direct and the mirror positions, into the
+// owner's rate-block buffer through distributed shared memory.  One cluster barrier per
+// block makes them visible, then each CTA runs the inverse DFT_Q of its own two rate pairs
+// (4 sequences) and writes W.  The two rate-block buffers alternate, so a CTA may write into
+// its peer's buffer for block i + 1 while the peer still transforms block i.
+// ------------------------------------------------------------------------------------
+// Forward DFT_Q for a two-CTA cluster (zdtf_czt_cl_kernel): CTA `rank` transforms only the A
+// rows of its own side (PC = 8 t pairs per chunk, 8 sequences in buf) and takes the mirror
+// values of the two-for-one unpacking from the CTA that holds the mirror side (itself for
+// residue pair 0), through distributed shared memory.  Two cluster barriers per chunk: the
+// peer's transforms are complete before they are read, and read before they are replaced.
+template <int Q, int NT, int T>
+__device__ __forceinline__ void czt_forward_cluster(const CztArgs& a, int c, const int* k1s, float2* buf,
+                                                    const float2* twt, float2* gs, float2* gnyq,
+                                                    int rank, cg::cluster_group& cluster) {
+  constexpr int SS = b_stride<Q>();
+  constexpr int PC = 8, QH = Q / 2;
+  constexpr int NE = PC * Q, NL = (NE + T - 1) / T;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < NT * QH; i += T) gs[i] = make_float2(0.f, 0.f);
+  if (c == 0 && rank == 0 && tid == 0)
+    for (int t = 0; t < NT; ++t) gnyq[t] = make_float2(0.f, 0.f);
+  const long long k1 = k1s[rank];
+  float2 v[NL];
+  auto load_chunk = [&](int p0) {
+#pragma unroll
+    for (int i = 0; i < NL; ++i) {
+      const int e = tid + i * T;
+      const int u = e / Q, na = e - u * Q;
+      const int pp = p0 + u;
+      v[i] = ((NE % T == 0 || e < NE) && pp < a.NP &&
+              FDR_DBG_OK(((long long)pp * a.P + k1) * Q + na < (long long)a.NP * a.P * Q))
+                 ? __ldcs(a.A + ((long long)pp * a.P + k1) * Q + na)
+                 : make_float2(0.f, 0.f);
+    }
+  };
+  load_chunk(0);
+  for (int p0 = 0; p0 < a.NP; p0 += PC) {
+    if (p0 > 0) cluster.sync();  // the peer has read this buffer's previous chunk
+#pragma unroll
+    for (int i = 0; i < NL; ++i) {
+      const int e = tid + i * T;
+      const int u = e / Q, na = e - u * Q;
+      if (NE % T == 0 || e < NE) buf[u * SS + pidx(na)] = v[i];
+    }
+    if (p0 + PC < a.NP) load_chunk(p0 + PC);
+    __syncthreads();
+    smem_fft<Q, PC, SS, T, -1>(buf, twt);
+    cluster.sync();  // both sides' transforms of this chunk are complete
+    for (int e = tid; e < PC * QH; e += T) {
+      const int u = e / QH, k2 = e - u * QH;
+      if (p0 + u >= a.NP) continue;
+      int ms, mk2;
+      mirror_of(c, rank, k2, Q, &ms, &mk2);
+      const float2* src = ms == rank ? buf : cluster.map_shared_rank(buf, ms);
+      const float2 zk = buf[u * SS + pidx(k2)];
+      const float2 zm = cconj(src[u * SS + pidx(mk2)]);
+      const float2 sm_ = cadd(zk, zm), d = csub(zk, zm);
+      const int t0 = 2 * (p0 + u);
+      gs_put(gs, QH, t0, k2, make_float2(0.5f * sm_.x, 0.5f * sm_.y));
+      if (t0 + 1 < NT) gs_put(gs, QH, t0 + 1, k2, make_float2(0.5f * d.y, -0.5f * d.x));
+    }
+    if (c == 0 && rank == 0 && tid == 0) {
+      for (int u = 0; u < PC && p0 + u < a.NP; ++u) {
+        const float2 z = buf[u * SS + pidx(Q / 2)];
+        const int t0 = 2 * (p0 + u);
+        gnyq[t0] = make_float2(z.x, 0.f);
+        if (t0 + 1 < NT) gnyq[t0 + 1] = make_float2(z.y, 0.f);
+      }
+    }
+  }
+  cluster.sync();  // every read of either buffer is done: they become rate-block buffers
+}
+
+struct CztClShape {
+  static constexpr int Q = 512, NT = 64, T = 512;
+  static constexpr int QH = Q / 2;                    // bins of one side (one CTA)
+  static constexpr int RG = 2 * T / QH;               // rate groups: 4 (128 bin pairs)
+  static constexpr int RT = kRatesPerBlock / RG;      // 2 rates (one rate pair) per thread
+  static constexpr int SS = b_stride<Q>();
+  static constexpr int TWT = kRatesPerBlock * SS;     // after the 8-sequence buffer
+  static constexpr int TWR = TWT + tw_size(Q);
+  static constexpr int GS_OFF = (TWR + 2 * Q + 1) & ~1;
+  static constexpr size_t SMEM = sizeof(float2) * (GS_OFF + NT * QH + NT);
+};
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CztClShape::T, 1)
+zdtf_czt_cl_kernel(CztArgs a) {
+  using SH = CztClShape;
+  constexpr int Q = SH::Q, NT = SH::NT, T = SH::T, QH = SH::QH, RT = SH::RT, SS = SH::SS;
+  static_assert(RT == 2, "one rate pair per thread");
+  cg::cluster_group cluster = cg::this_cluster();
+  extern __shared__ float2 sm[];
+  float2* const buf = sm;  // forward pass: 8 sequences; then two rate-block buffers of 4
+  float2* const twt = sm + SH::TWT;
+  float2* const twr = sm + SH::TWR;
+  float2* const gs = sm + SH::GS_OFF;
+  float2* const gnyq = gs + NT * QH;
+  const int tid = threadIdx.x;
+  const int rank = (int)cluster.block_rank();  // the side this CTA holds
+  const int c = blockIdx.x >> 1;                // residue pair
+  const int P = a.P;
+  const int k1s[2] = {c == 0 ? 0 : c, c == 0 ? P / 2 : P - c};
+  const float invN = 1.0f / (float)a.N;
+  for (int i = tid; i < tw_size(Q); i += T) twt[i] = __ldg(a.tab.twQ + i);
+  for (int i = tid; i < 2 * Q; i += T) {
+    const int sd = i / Q, na = i - sd * Q;
+    twr[i] = cscale(cconj(tw_fwd(a.tab, (long long)k1s[sd] * na)), invN);
+  }
+  czt_forward_cluster<Q, NT, T>(a, c, k1s, buf, twt, gs, gnyq, rank, cluster);
+
+  // thread -> (bin pair bp of this side, rate pair rg of every block)
+  const int bp = tid % (QH / 2), rg = tid / (QH / 2);
+  const int side = rank, k20 = 2 * bp;
+  int ms[2], mk2[2];
+  mirror_of(c, side, k20, Q, &ms[0], &mk2[0]);
+  mirror_of(c, side, k20 + 1, Q, &ms[1], &mk2[1]);
+  const bool dc = (c == 0 && side == 0 && k20 == 0);  // lane 0 is the DC bin
+  const unsigned long long mask = a.ph.mask;
+  unsigned long long alpha[2], beta[2];
+  float2 pwx, pwy;  // exact w(k_lane, dr) (lanes = the two bins)
+  float2 win;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const unsigned long long k = (unsigned long long)k1s[side] + (unsigned long long)P * (k20 + h);
+    alpha[h] = (k * a.ph.R0) & mask;
+    beta[h] = (k * a.ph.Rd) & mask;
+    const float2 p = cis_phase(beta[h] & mask, a.ph);
+    if (h == 0) { pwx.x = p.x; pwy.x = p.y; } else { pwx.y = p.x; pwy.y = p.y; }
+    const float wv = window_value(a, (long long)k);
+    if (h == 0) win.x = wv; else win.y = wv;
+  }
+  const unsigned long long kny = (unsigned long long)(a.N / 2);
+  const unsigned long long alpha_n = (kny * a.ph.R0) & mask, beta_n = (kny * a.ph.Rd) & mask;
+  const int Nt = a.Nt;
+  const float4* gs4 = reinterpret_cast<const float4*>(gs);
+  const int owner = rg >> 1, ul = rg & 1;  // this thread's rate pair: owner CTA, pair there
+  const int k1a = k1s[0], k1b = k1s[1];
+
+  const int q_begin = blockIdx.y * a.pairs_per_group;
+  const int q_end = min(a.npairs, q_begin + a.pairs_per_group);
+  const int nblk = q_end > q_begin ? (q_end - q_begin + kRatesPerBlock / 2 - 1) / (kRatesPerBlock / 2) : 0;
+  for (int ib = 0; ib < nblk; ++ib) {
+    const int q0 = q_begin + ib * (kRatesPerBlock / 2);
+    float2* const hb_local = buf + (ib & 1) * 4 * SS;
+    float2* const hb = owner == rank ? hb_local : cluster.map_shared_rank(hb_local, owner);
+    const int j0 = 2 * q0 + rg * RT;  // this thread's first rate of the block
+    const long long jb = a.blk_base ? (long long)__ldg(a.blk_base + (q0 >> 2)) : (long long)(2 * q0);
+    float2 Sx[2], Sy[2];
+    if (j0 < a.Nr) {  // uniform over the warp (rg is)
+      float2 W0x, W0y;
+      {
+        const unsigned long long jj = (unsigned long long)(jb + rg * RT);
+        const float2 w0 = cis_phase((alpha[0] + jj * beta[0]) & mask, a.ph);
+        const float2 w1 = cis_phase((alpha[1] + jj * beta[1]) & mask, a.ph);
+        W0x = make_float2(w0.x, w1.x);
+        W0y = make_float2(w0.y, w1.y);
+      }
+      const float2 NW0y = pk_neg(W0y);
+      float2 Wx[2], Wy[2], NWy[2];
+      Wx[0] = W0x;
+      Wy[0] = W0y;
+      Wx[1] = pk_fma(W0x, pwx, pk_mul(NW0y, pwy));
+      Wy[1] = pk_fma(W0x, pwy, pk_mul(W0y, pwx));
+      NWy[0] = NW0y;
+      NWy[1] = pk_neg(Wy[1]);
+      const float4 gl = gs4[(Nt - 1) * (QH / 2) + bp];
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        Sx[r] = make_float2(gl.x, gl.y);
+        Sy[r] = make_float2(gl.z, gl.w);
+      }
+#pragma unroll 4
+      for (int t = Nt - 2; t >= 0; --t) {
+        const float4 gt = gs4[t * (QH / 2) + bp];
+        const float2 gx = make_float2(gt.x, gt.y), gy = make_float2(gt.z, gt.w);
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+          const float2 tx = pk_fma(Sx[r], Wx[r], pk_fma(Sy[r], NWy[r], gx));
+          const float2 ty = pk_fma(Sx[r], Wy[r], pk_fma(Sy[r], Wx[r], gy));
+          Sx[r] = tx;
+          Sy[r] = ty;
+        }
+      }
+    } else {
+      Sx[0] = Sx[1] = Sy[0] = Sy[1] = make_float2(0.f, 0.f);
+    }
+    const bool ok_a = j0 < a.Nr, ok_b = j0 + 1 < a.Nr;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const float wh = h ? win.y : win.x;
+      const float2 sa = ok_a ? cscale(make_float2(h ? Sx[0].y : Sx[0].x, h ? Sy[0].y : Sy[0].x), wh)
+                             : make_float2(0.f, 0.f);
+      const float2 sb = ok_b ? cscale(make_float2(h ? Sx[1].y : Sx[1].x, h ? Sy[1].y : Sy[1].x), wh)
+                             : make_float2(0.f, 0.f);
+      if (dc && h == 0) {
+        hb[(2 * ul) * SS + pidx(0)] = make_float2(sa.x, sb.x);
+      } else {
+        hb[(2 * ul + side) * SS + pidx(k20 + h)] = make_float2(sa.x - sb.y, sa.y + sb.x);
+        hb[(2 * ul + ms[h]) * SS + pidx(mk2[h])] = make_float2(sa.x + sb.y, sb.x - sa.y);
+      }
+    }
+    if (c == 0 && rank == 0 && tid == 0) {  // the real-only Nyquist bin of every rate of the block
+      const float wn = window_value(a, (long long)kny);
+      for (int u = 0; u < kRatesPerBlock / 2; ++u) {
+        float v[2];
+        for (int hh = 0; hh < 2; ++hh) {
+          const int j = 2 * q0 + 2 * u + hh;
+          const float2 wv = cis_phase((alpha_n + (unsigned long long)(jb + 2 * u + hh) * beta_n) & mask, a.ph);
+          float2 sv = gnyq[Nt - 1];
+          for (int t = Nt - 2; t >= 0; --t)
+            sv = make_float2(fmaf(sv.x, wv.x, fmaf(-sv.y, wv.y, gnyq[t].x)),
+                             fmaf(sv.x, wv.y, fmaf(sv.y, wv.x, gnyq[t].y)));
+          v[hh] = (j < a.Nr) ? sv.x * wn : 0.f;
+        }
+        float2* const hbo = (u >> 1) == rank ? hb_local : cluster.map_shared_rank(hb_local, u >> 1);
+        hbo[(2 * (u & 1)) * SS + pidx(Q / 2)] = make_float2(v[0], v[1]);
+      }
+    }
+    cluster.sync();  // the block's sums, local and remote, are in the owners' buffers
+    // the inverse DFT_Q of this CTA's rate pairs 2*rank and 2*rank + 1; the last pass writes W
+    float2* const Wq = a.W + (long long)q0 * P * Q;  // 32-bit offsets below (Nf <= 2^22)
+    smem_fft_emit<Q, 4, SS, T, +1>(hb_local, twt, [&](int ls, int na, float2 v) {
+      const int p = 2 * rank + (ls >> 1), sd = ls & 1;
+      const unsigned off = (unsigned)((p * P + (sd ? k1b : k1a)) * Q + na);
+      if (q0 + p < q_end && FDR_DBG_OK((long long)q0 * P * Q + off < (long long)a.npairs * P * Q))
+        Wq[off] = cmul(v, twr[sd * Q + na]);
+    });
+  }
+}
+
+// A -> F (reference layout K x Nt) for the split of zdtf_czt_cl_kernel: CTA 2c + s writes the
+// F of side s of residue pair c (no cluster: the two sides are independent here).
+__global__ void __launch_bounds__(CztClShape::T, 1) zdtf_a2f_half_kernel(CztArgs a) {
+  using SH = CztClShape;
+  constexpr int Q = SH::Q, NT = SH::NT, T = SH::T, QH = SH::QH;
+  extern __shared__ float2 sm[];
+  float2* const buf = sm;
+  float2* const twt = sm + SH::TWT;
+  float2* const gs = sm + SH::GS_OFF;
+  float2* const gnyq = gs + NT * QH;
+  const int tid = threadIdx.x;
+  const int side = blockIdx.x & 1, c = blockIdx.x >> 1;
+  const int P = a.P;
+  const int k1s[2] = {c == 0 ? 0 : c, c == 0 ? P / 2 : P - c};
+  for (int i = tid; i < tw_size(Q); i += T) twt[i] = __ldg(a.tab.twQ + i);
+  czt_forward_smem<Q, NT, T, true>(a, c, k1s, buf, twt, gs, gnyq, side);
+  const long long K = a.N / 2 + 1;
+  for (int e = tid; e < QH * a.Nt; e += T) {
+    const int t = e / QH, k2 = e - t * QH;
+    if (FDR_DBG_OK((long long)k1s[side] + (long long)P * k2 + t * K < K * a.Nt))
+      a.F[(long long)k1s[side] + (long long)P * k2 + t * K] = gs_get(gs, QH, t, k2);
+  }
+  if (c == 0 && side == 0 && tid == 0)
+    for (int t = 0; t < a.Nt; ++t) a.F[a.N / 2 + t * K] = gnyq[t];
 }
 
 template <int Q, int NT>
@@ -1840,7 +2111,10 @@ struct CztShape {  // buf | twt | twr | gnyq | buf2 (the second rate-block buffe
 // mixed-precision output pass, whose tensor-core DFTs are written for P = 1024) keeps 1024
 // bins per CTA for Nt <= 16, so that Nf = 2^20 splits as 1024 x 1024.
 static int fused_qlog(int L, int64_t Nt, bool p1024 = false) {
-  const int cap = Nt <= 16 ? ((L <= 20 && !p1024) ? 9 : 10) : (Nt <= 32 ? 9 : 8);
+  // 32 < Nt <= 64 at Nf = 2^20, 2^21: 512 bins per residue pair, F split over a cluster of two
+  // CTAs (zdtf_czt_cl_kernel), so that P stays 2048 / 4096
+  const int cap = Nt <= 16 ? ((L <= 20 && !p1024) ? 9 : 10)
+                           : (Nt <= 32 ? 9 : ((L == 20 || L == 21) ? 9 : 8));
   return std::min(cap, (L + 1) / 2);
 }
 
@@ -1991,6 +2265,10 @@ static int set_smem_attrs() {
                                 (int)CztWsShape<Q>::template smem<NT>()));
   SET_WS(512, 32) SET_WS(256, 32) SET_WS(256, 64)
 #undef SET_WS
+  FDR_CUDA(cudaFuncSetAttribute(zdtf_czt_cl_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)CztClShape::SMEM));
+  FDR_CUDA(cudaFuncSetAttribute(zdtf_a2f_half_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)CztClShape::SMEM));
   if (dev < 64) done[dev] = true;
   return FDR_OK;
 }
@@ -2090,6 +2368,11 @@ int fused_a2f(const FusedPlan* st, const float2* A, float2* F, cudaStream_t s) {
   CztArgs a = czt_args(st, A, nullptr);
   a.F = F;
   const int Q = st->Q, ctas = st->P / 2;
+  if (st->Nt > 32 && Q == CztClShape::Q) {
+    zdtf_a2f_half_kernel<<<2 * ctas, CztClShape::T, CztClShape::SMEM, s>>>(a);
+    FDR_LAUNCH_CHECK("zdtf_a2f_half_kernel");
+    return FDR_OK;
+  }
   if (st->Nt > kFusedMaxNt) {
     const int NT = st->Nt <= 32 ? 32 : 64;
 #define LAUNCH_A2FS(QQ, NN)                                                                    \
@@ -2153,6 +2436,11 @@ int fused_czt_blocks(const FusedPlan* st, const float2* A, float2* W, float r0, 
   ppg = (int)cdiv(ppg, kRatesPerBlock / 2) * (kRatesPerBlock / 2);
   groups = (int)cdiv(st->npairs, ppg);
   a.pairs_per_group = ppg;
+  if (st->Nt > 32 && Q == CztClShape::Q) {  // F of 64 steps for 512 bins: two-CTA cluster
+    zdtf_czt_cl_kernel<<<dim3(2 * ctas, groups), CztClShape::T, CztClShape::SMEM, s>>>(a);
+    FDR_LAUNCH_CHECK("zdtf_czt_cl_kernel");
+    return FDR_OK;
+  }
   // 16 < Nt <= 64 with 256 or 512 bins per CTA: the warp-specialised kernel (measured 6-9%
   // faster than zdtf_czt_smem_kernel at Nf = 2^19..2^20); Nt <= 16 keeps F in registers.
   if (st->Nt > kFusedMaxNt && ((Q == 512 && st->Nt <= 32) || (Q == 256 && st->Nt <= 64))) {

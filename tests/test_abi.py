@@ -62,7 +62,8 @@ def test_fused_split_plan(fdr):
     """The four-step split of the fused path, chosen on the host: 512 bins per czt CTA up to
     Nf = 2^20 with F in registers (Nt <= 16), 1024 above and for mixed-precision workspaces
     at 2^20 (their tensor-core output pass is written for P = 1024), 512 / 256 bins with F
-    in shared memory (Nt <= 32 / 64); the staged kernels outside 2^12..2^22 or P > 4096."""
+    in shared memory (Nt <= 32 / 64), and 512 bins at Nf = 2^20 and 2^21 for 32 < Nt <= 64
+    (F split over a two-CTA cluster); the staged kernels outside 2^12..2^22 or P > 4096."""
     fs = fdr.fused_split
     assert fs(2 ** 20, 16, 129) == (2048, 512)
     assert fs(2 ** 20, 16, 129, mixed_precision=True) == (1024, 1024)
@@ -70,7 +71,9 @@ def test_fused_split_plan(fdr):
     assert fs(2 ** 21, 16, 17) == (2048, 1024)
     assert fs(2 ** 22, 16, 17) == (4096, 1024)
     assert fs(2 ** 20, 24, 33) == (2048, 512)
-    assert fs(2 ** 20, 64, 65) == (4096, 256)
+    assert fs(2 ** 20, 64, 65) == (2048, 512)
+    assert fs(2 ** 21, 33, 9) == (4096, 512)
+    assert fs(2 ** 19, 64, 65) == (2048, 256)
     assert fs(2 ** 18, 40, 33) == (1024, 256)
     assert fs(2 ** 12, 16, 17) == (64, 64)
     for Nf, Nt in ((2 ** 23, 16), (2 ** 11, 16), (3 * 2 ** 18, 16), (2 ** 20, 65), (2 ** 22, 64)):
