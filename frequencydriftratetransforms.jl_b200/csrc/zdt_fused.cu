@@ -1090,7 +1090,7 @@ struct CztClShape {
   static constexpr int RG = 2 * T / QH;               // rate groups: 4 (128 bin pairs)
   static constexpr int RT = kRatesPerBlock / RG;      // 2 rates (one rate pair) per thread
   static constexpr int SS = b_stride<Q>();
-  static constexpr int TWT = kRatesPerBlock * SS;     // after the 8-sequence buffer
+  static constexpr int TWT = 2 * kRatesPerBlock * SS;  // after two 8-sequence buffers
   static constexpr int TWR = TWT + tw_size(Q);
   static constexpr int GS_OFF = (TWR + 2 * Q + 1) & ~1;
   static constexpr size_t SMEM = sizeof(float2) * (GS_OFF + NT * QH + NT);
@@ -1103,7 +1103,7 @@ zdtf_czt_cl_kernel(CztArgs a) {
   static_assert(RT == 2, "one rate pair per thread");
   cg::cluster_group cluster = cg::this_cluster();
   extern __shared__ float2 sm[];
-  float2* const buf = sm;  // forward pass: 8 sequences; then two rate-block buffers of 4
+  float2* const buf = sm;  // forward pass: 8 sequences; then two buffers of 8 (two rate blocks)
   float2* const twt = sm + SH::TWT;
   float2* const twr = sm + SH::TWR;
   float2* const gs = sm + SH::GS_OFF;
@@ -1152,91 +1152,104 @@ zdtf_czt_cl_kernel(CztArgs a) {
   const int q_begin = blockIdx.y * a.pairs_per_group;
   const int q_end = min(a.npairs, q_begin + a.pairs_per_group);
   const int nblk = q_end > q_begin ? (q_end - q_begin + kRatesPerBlock / 2 - 1) / (kRatesPerBlock / 2) : 0;
-  for (int ib = 0; ib < nblk; ++ib) {
-    const int q0 = q_begin + ib * (kRatesPerBlock / 2);
-    float2* const hb_local = buf + (ib & 1) * 4 * SS;
-    float2* const hb = owner == rank ? hb_local : cluster.map_shared_rank(hb_local, owner);
-    const int j0 = 2 * q0 + rg * RT;  // this thread's first rate of the block
-    const long long jb = a.blk_base ? (long long)__ldg(a.blk_base + (q0 >> 2)) : (long long)(2 * q0);
-    float2 Sx[2], Sy[2];
-    if (j0 < a.Nr) {  // uniform over the warp (rg is)
-      float2 W0x, W0y;
-      {
-        const unsigned long long jj = (unsigned long long)(jb + rg * RT);
-        const float2 w0 = cis_phase((alpha[0] + jj * beta[0]) & mask, a.ph);
-        const float2 w1 = cis_phase((alpha[1] + jj * beta[1]) & mask, a.ph);
-        W0x = make_float2(w0.x, w1.x);
-        W0y = make_float2(w0.y, w1.y);
-      }
-      const float2 NW0y = pk_neg(W0y);
-      float2 Wx[2], Wy[2], NWy[2];
-      Wx[0] = W0x;
-      Wy[0] = W0y;
-      Wx[1] = pk_fma(W0x, pwx, pk_mul(NW0y, pwy));
-      Wy[1] = pk_fma(W0x, pwy, pk_mul(W0y, pwx));
-      NWy[0] = NW0y;
-      NWy[1] = pk_neg(Wy[1]);
-      const float4 gl = gs4[(Nt - 1) * (QH / 2) + bp];
-#pragma unroll
-      for (int r = 0; r < 2; ++r) {
-        Sx[r] = make_float2(gl.x, gl.y);
-        Sy[r] = make_float2(gl.z, gl.w);
-      }
-#pragma unroll 4
-      for (int t = Nt - 2; t >= 0; --t) {
-        const float4 gt = gs4[t * (QH / 2) + bp];
-        const float2 gx = make_float2(gt.x, gt.y), gy = make_float2(gt.z, gt.w);
+  // two rate blocks per cluster barrier: 8 sequences per buffer ([block 0: 4][block 1: 4])
+  const int nsb = (nblk + 1) / 2;
+  for (int isb = 0; isb < nsb; ++isb) {
+    float2* const hb_local = buf + (isb & 1) * kRatesPerBlock * SS;  // 8 sequences
+    float2* const hb_owner = owner == rank ? hb_local : cluster.map_shared_rank(hb_local, owner);
+#pragma unroll 1
+    for (int bb = 0; bb < 2; ++bb) {
+      const int ib = 2 * isb + bb;
+      const bool live = ib < nblk;  // an odd last block leaves the second half unused
+      const int q0 = q_begin + ib * (kRatesPerBlock / 2);
+      float2* const hb = hb_owner + bb * 4 * SS;
+      const int j0 = 2 * q0 + rg * RT;  // this thread's first rate of the block
+      const long long jb = !live ? 0 : a.blk_base ? (long long)__ldg(a.blk_base + (q0 >> 2)) : (long long)(2 * q0);
+      float2 Sx[2], Sy[2];
+      if (live && j0 < a.Nr) {  // uniform over the warp (rg is)
+        float2 W0x, W0y;
+        {
+          const unsigned long long jj = (unsigned long long)(jb + rg * RT);
+          const float2 w0 = cis_phase((alpha[0] + jj * beta[0]) & mask, a.ph);
+          const float2 w1 = cis_phase((alpha[1] + jj * beta[1]) & mask, a.ph);
+          W0x = make_float2(w0.x, w1.x);
+          W0y = make_float2(w0.y, w1.y);
+        }
+        const float2 NW0y = pk_neg(W0y);
+        float2 Wx[2], Wy[2], NWy[2];
+        Wx[0] = W0x;
+        Wy[0] = W0y;
+        Wx[1] = pk_fma(W0x, pwx, pk_mul(NW0y, pwy));
+        Wy[1] = pk_fma(W0x, pwy, pk_mul(W0y, pwx));
+        NWy[0] = NW0y;
+        NWy[1] = pk_neg(Wy[1]);
+        const float4 gl = gs4[(Nt - 1) * (QH / 2) + bp];
 #pragma unroll
         for (int r = 0; r < 2; ++r) {
-          const float2 tx = pk_fma(Sx[r], Wx[r], pk_fma(Sy[r], NWy[r], gx));
-          const float2 ty = pk_fma(Sx[r], Wy[r], pk_fma(Sy[r], Wx[r], gy));
-          Sx[r] = tx;
-          Sy[r] = ty;
+          Sx[r] = make_float2(gl.x, gl.y);
+          Sy[r] = make_float2(gl.z, gl.w);
         }
-      }
-    } else {
-      Sx[0] = Sx[1] = Sy[0] = Sy[1] = make_float2(0.f, 0.f);
-    }
-    const bool ok_a = j0 < a.Nr, ok_b = j0 + 1 < a.Nr;
+#pragma unroll 4
+        for (int t = Nt - 2; t >= 0; --t) {
+          const float4 gt = gs4[t * (QH / 2) + bp];
+          const float2 gx = make_float2(gt.x, gt.y), gy = make_float2(gt.z, gt.w);
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const float wh = h ? win.y : win.x;
-      const float2 sa = ok_a ? cscale(make_float2(h ? Sx[0].y : Sx[0].x, h ? Sy[0].y : Sy[0].x), wh)
-                             : make_float2(0.f, 0.f);
-      const float2 sb = ok_b ? cscale(make_float2(h ? Sx[1].y : Sx[1].x, h ? Sy[1].y : Sy[1].x), wh)
-                             : make_float2(0.f, 0.f);
-      if (dc && h == 0) {
-        hb[(2 * ul) * SS + pidx(0)] = make_float2(sa.x, sb.x);
-      } else {
-        hb[(2 * ul + side) * SS + pidx(k20 + h)] = make_float2(sa.x - sb.y, sa.y + sb.x);
-        hb[(2 * ul + ms[h]) * SS + pidx(mk2[h])] = make_float2(sa.x + sb.y, sb.x - sa.y);
-      }
-    }
-    if (c == 0 && rank == 0 && tid == 0) {  // the real-only Nyquist bin of every rate of the block
-      const float wn = window_value(a, (long long)kny);
-      for (int u = 0; u < kRatesPerBlock / 2; ++u) {
-        float v[2];
-        for (int hh = 0; hh < 2; ++hh) {
-          const int j = 2 * q0 + 2 * u + hh;
-          const float2 wv = cis_phase((alpha_n + (unsigned long long)(jb + 2 * u + hh) * beta_n) & mask, a.ph);
-          float2 sv = gnyq[Nt - 1];
-          for (int t = Nt - 2; t >= 0; --t)
-            sv = make_float2(fmaf(sv.x, wv.x, fmaf(-sv.y, wv.y, gnyq[t].x)),
-                             fmaf(sv.x, wv.y, fmaf(sv.y, wv.x, gnyq[t].y)));
-          v[hh] = (j < a.Nr) ? sv.x * wn : 0.f;
+          for (int r = 0; r < 2; ++r) {
+            const float2 tx = pk_fma(Sx[r], Wx[r], pk_fma(Sy[r], NWy[r], gx));
+            const float2 ty = pk_fma(Sx[r], Wy[r], pk_fma(Sy[r], Wx[r], gy));
+            Sx[r] = tx;
+            Sy[r] = ty;
+          }
         }
-        float2* const hbo = (u >> 1) == rank ? hb_local : cluster.map_shared_rank(hb_local, u >> 1);
-        hbo[(2 * (u & 1)) * SS + pidx(Q / 2)] = make_float2(v[0], v[1]);
+      } else {
+        Sx[0] = Sx[1] = Sy[0] = Sy[1] = make_float2(0.f, 0.f);
+      }
+      const bool ok_a = live && j0 < a.Nr, ok_b = live && j0 + 1 < a.Nr;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const float wh = h ? win.y : win.x;
+        const float2 sa = ok_a ? cscale(make_float2(h ? Sx[0].y : Sx[0].x, h ? Sy[0].y : Sy[0].x), wh)
+                               : make_float2(0.f, 0.f);
+        const float2 sb = ok_b ? cscale(make_float2(h ? Sx[1].y : Sx[1].x, h ? Sy[1].y : Sy[1].x), wh)
+                               : make_float2(0.f, 0.f);
+        if (dc && h == 0) {
+          hb[(2 * ul) * SS + pidx(0)] = make_float2(sa.x, sb.x);
+        } else {
+          hb[(2 * ul + side) * SS + pidx(k20 + h)] = make_float2(sa.x - sb.y, sa.y + sb.x);
+          hb[(2 * ul + ms[h]) * SS + pidx(mk2[h])] = make_float2(sa.x + sb.y, sb.x - sa.y);
+        }
+      }
+      if (c == 0 && rank == 0 && tid == 0) {  // the real-only Nyquist bin of every rate of the block
+        const float wn = window_value(a, (long long)kny);
+        for (int u = 0; u < kRatesPerBlock / 2; ++u) {
+          float v[2];
+          for (int hh = 0; hh < 2; ++hh) {
+            const int j = 2 * q0 + 2 * u + hh;
+            float2 sv = make_float2(0.f, 0.f);
+            if (live) {
+              const float2 wv = cis_phase((alpha_n + (unsigned long long)(jb + 2 * u + hh) * beta_n) & mask, a.ph);
+              sv = gnyq[Nt - 1];
+              for (int t = Nt - 2; t >= 0; --t)
+                sv = make_float2(fmaf(sv.x, wv.x, fmaf(-sv.y, wv.y, gnyq[t].x)),
+                                 fmaf(sv.x, wv.y, fmaf(sv.y, wv.x, gnyq[t].y)));
+            }
+            v[hh] = (live && j < a.Nr) ? sv.x * wn : 0.f;
+          }
+          float2* const hbo = ((u >> 1) == rank ? hb_local : cluster.map_shared_rank(hb_local, u >> 1)) + bb * 4 * SS;
+          hbo[(2 * (u & 1)) * SS + pidx(Q / 2)] = make_float2(v[0], v[1]);
+        }
       }
     }
-    cluster.sync();  // the block's sums, local and remote, are in the owners' buffers
-    // the inverse DFT_Q of this CTA's rate pairs 2*rank and 2*rank + 1; the last pass writes W
-    float2* const Wq = a.W + (long long)q0 * P * Q;  // 32-bit offsets below (Nf <= 2^22)
-    smem_fft_emit<Q, 4, SS, T, +1>(hb_local, twt, [&](int ls, int na, float2 v) {
-      const int p = 2 * rank + (ls >> 1), sd = ls & 1;
+    cluster.sync();  // both blocks' sums, local and remote, are in the owners' buffers
+    // the inverse DFT_Q of this CTA's rate pairs 2*rank, 2*rank + 1 of both blocks (8
+    // sequences); the last pass writes W
+    smem_fft_emit<Q, 2 * kRatesPerBlock / 2, SS, T, +1>(hb_local, twt, [&](int ls, int na, float2 v) {
+      const int bb = ls >> 2, lq = ls & 3;
+      const int q0 = q_begin + (2 * isb + bb) * (kRatesPerBlock / 2);
+      const int p = 2 * rank + (lq >> 1), sd = lq & 1;
       const unsigned off = (unsigned)((p * P + (sd ? k1b : k1a)) * Q + na);
       if (q0 + p < q_end && FDR_DBG_OK((long long)q0 * P * Q + off < (long long)a.npairs * P * Q))
-        Wq[off] = cmul(v, twr[sd * Q + na]);
+        a.W[(long long)q0 * P * Q + off] = cmul(v, twr[sd * Q + na]);
     });
   }
 }
