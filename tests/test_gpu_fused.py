@@ -22,7 +22,9 @@ def _spec(oracle, Nf, Nt, seed, ntones=3):
     (2 ** 21, 4, -1.0, 0.25, 9), (2 ** 22, 2, 0.5, 1.0, 3),
     # F in shared memory (16 < Nt <= 64)
     (4096, 32, -2.0, 1 / 16, 65), (2 ** 14, 17, -1.0, 0.25, 9), (2 ** 16, 64, -2.0, 1 / 16, 65),
-    (2 ** 18, 33, -8.0, 1 / 16, 257), (2 ** 20, 64, -2.0, 1 / 16, 3)])
+    (2 ** 18, 33, -8.0, 1 / 16, 257), (2 ** 20, 64, -2.0, 1 / 16, 3),
+    # 32 < Nt <= 64 at 2^20 and 2^21: two-CTA cluster czt kernel
+    (2 ** 20, 40, 1.0, 0.25, 17), (2 ** 21, 36, -2.0, 1 / 16, 3)])
 def test_fused_vs_truth_and_staged(fdr, oracle, Nf, Nt, r0, dr, Nr):
     spec = _spec(oracle, Nf, Nt, seed=Nf + Nt)
     ws = fdr.ZDTWorkspace(spec, r0, dr, Nr)
@@ -79,10 +81,12 @@ def test_fused_windows_and_batches(fdr, oracle):
         assert oracle.rel_linf(d.cpu().numpy(), truth) < 1e-5
 
 
-@pytest.mark.parametrize("Nf,Nt,Nr", [(2 ** 16, 32, 41), (2 ** 17, 64, 65), (2 ** 15, 24, 9), (2 ** 19, 20, 17)])
+@pytest.mark.parametrize("Nf,Nt,Nr", [(2 ** 16, 32, 41), (2 ** 17, 64, 65), (2 ** 15, 24, 9), (2 ** 19, 20, 17),
+                                       (2 ** 20, 48, 9)])
 def test_fused_windows_and_batches_shared_memory_f(fdr, oracle, Nf, Nt, Nr):
-    """16 < Nt <= 64 with 256 or 512 bins per czt CTA (the warp-specialised czt kernel):
-    Hamming and custom windows and an r0 list against the staged kernels and FP64."""
+    """16 < Nt <= 64 with 256 or 512 bins per czt CTA (the warp-specialised czt kernel, and
+    the two-CTA cluster kernel at Nf = 2^20 with Nt > 32): Hamming and custom windows and an
+    r0 list against the staged kernels and FP64."""
     P, Q = fdr.fused_split(Nf, Nt, Nr)
     assert Q in (256, 512)
     spec = _spec(oracle, Nf, Nt, seed=3 * Nf + Nt)
