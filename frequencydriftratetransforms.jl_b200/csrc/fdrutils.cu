@@ -846,21 +846,22 @@ int fdr_stats(const float* const* fdrs, int64_t nb, int64_t Nf, int64_t Nrb, dou
   FDR_CHECK_ARG(nb >= 1 && Nf >= 1 && Nrb >= 1, "fdrstats: bad sizes");
   for (int64_t b = 0; b < nb; ++b) FDR_CHECK_ARG(fdrs[b] != nullptr, "fdrstats: matrix %lld is NULL", (long long)b);
   cudaStream_t s = (cudaStream_t)stream;
+  // The finalize kernel writes (m, s) straight into mapped pinned words: no device-to-host
+  // copy that would queue behind the copy engine's other work.
+  void *ms_host = nullptr, *ms_dev = nullptr;
+  FDR_TRY(pinned_staging(3 * sizeof(double), &ms_host, &ms_dev));
   void** d_mats = nullptr;
-  double* d_ms = nullptr;
   FDR_TRY(upload_ptrs((const void* const*)fdrs, nb, &d_mats, s));
-  FDR_TRY(scratch_alloc((void**)&d_ms, 3 * sizeof(double), s));
-  int st = stats_device((const float* const*)d_mats, nb, Nf, Nrb, d_ms, 0, 0.0, s);
-  double h[2] = {0, 0};
+  int st = stats_device((const float* const*)d_mats, nb, Nf, Nrb, static_cast<double*>(ms_dev), 0,
+                        0.0, s);
   if (st == FDR_OK) {
-    cudaError_t e = cudaMemcpyAsync(h, d_ms, sizeof(h), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) st = cuda_status(e, "fdrstats copy");
+    const cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) st = cuda_status(e, "fdrstats");
   }
-  scratch_free(d_ms, s);
   scratch_free(d_mats, s);
-  *m = h[0];
-  *s_out = h[1];
+  const volatile double* h = static_cast<const volatile double*>(ms_host);
+  *m = st == FDR_OK ? h[0] : 0.0;
+  *s_out = st == FDR_OK ? h[1] : 0.0;
   return st;
 }
 

@@ -114,7 +114,10 @@ __global__ void block_sums_kernel(const int* __restrict__ flag, long long n, int
   }
 }
 
-__global__ void scan_bsums_kernel(int* __restrict__ bsum, long long nb, long long* __restrict__ total) {
+// result[0] receives the cluster total and result[1] the error flags that the earlier kernels
+// of the stream left in *err (result is a mapped host word pair, read after the stream syncs).
+__global__ void scan_bsums_kernel(int* __restrict__ bsum, long long nb, const int* __restrict__ err,
+                                  long long* __restrict__ result) {
   // one CTA of kCluThreads threads; each thread scans a contiguous chunk
   __shared__ long long part[kCluThreads];
   const long long per = (nb + kCluThreads - 1) / kCluThreads;
@@ -126,7 +129,8 @@ __global__ void scan_bsums_kernel(int* __restrict__ bsum, long long nb, long lon
   if (threadIdx.x == 0) {
     long long run = 0;
     for (int k = 0; k < kCluThreads; ++k) { const long long v = part[k]; part[k] = run; run += v; }
-    *total = run;
+    result[0] = run;
+    result[1] = *err;
   }
   __syncthreads();
   long long run = part[threadIdx.x];
@@ -247,15 +251,15 @@ int fdr_cluster_protohits(const int64_t* hits, int64_t nhits, int64_t Nf, int64_
   cudaStream_t s = (cudaStream_t)stream;
   const long long n = nhits;
   const unsigned grid = (unsigned)cdiv(n, kCluThreads);
-  // scratch: parent, root, flag, cid (n ints each), block sums, the error flags, then the
-  // cluster total in an 8-byte aligned slot
+  // scratch: parent, root, flag, cid (n ints each), block sums, then the error flags; the
+  // total and the flags come back through mapped pinned words, not a device-to-host copy
   const size_t ints = 4 * (size_t)n + grid + 1;
-  const size_t total_off = (sizeof(int) * ints + 7) & ~(size_t)7;
+  void *res_host = nullptr, *res_dev = nullptr;
+  FDR_TRY(pinned_staging(2 * sizeof(long long), &res_host, &res_dev));
   int* w = nullptr;
-  FDR_TRY(scratch_alloc((void**)&w, total_off + sizeof(long long), s));
+  FDR_TRY(scratch_alloc((void**)&w, sizeof(int) * ints, s));
   int *parent = w, *root = w + n, *flag = w + 2 * n, *cid = w + 3 * n, *bsum = w + 4 * n;
   int* err = bsum + grid;
-  long long* d_total = (long long*)((char*)w + total_off);
   int st = FDR_OK;
   void** d_mats = nullptr;
   unsigned long long* peak = nullptr;
@@ -270,17 +274,20 @@ int fdr_cluster_protohits(const int64_t* hits, int64_t nhits, int64_t Nf, int64_
     link_kernel<<<grid, kCluThreads, 0, s>>>((const long long*)hits, n, Nf, di, dj, parent, err);
     flatten_kernel<<<grid, kCluThreads, 0, s>>>(parent, n, root, flag);
     block_sums_kernel<<<grid, kCluThreads, 0, s>>>(flag, n, bsum);
-    scan_bsums_kernel<<<1, kCluThreads, 0, s>>>(bsum, grid, d_total);
+    scan_bsums_kernel<<<1, kCluThreads, 0, s>>>(bsum, grid, err, static_cast<long long*>(res_dev));
     block_scan_kernel<<<grid, kCluThreads, 0, s>>>(flag, n, bsum, cid);
     count_launch(7);
     e = cudaPeekAtLastError();
     if (e != cudaSuccess) st = cuda_status(e, "cluster kernels");
   }
   if (st == FDR_OK) {
-    e = cudaMemcpyAsync(&h_total, d_total, sizeof(long long), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) st = cuda_status(e, "cluster count");
+  }
+  if (st == FDR_OK) {
+    const volatile long long* r = static_cast<const volatile long long*>(res_host);
+    h_total = r[0];
+    h_err = (int)r[1];
   }
   if (st == FDR_OK && (h_err & 3)) {
     set_error(FDR_ERR_INVALID_ARGUMENT, "cluster_protohits: hits must be in range and in column-major "
