@@ -355,7 +355,7 @@ int fdr_zdt_fused_split(int64_t Nf, int64_t Nt, int64_t Nr, uint32_t flags, int6
     return FDR_ERR_UNSUPPORTED_SIZE;
   }
   int pl = 0, ql = 0;
-  fused_split_log2(Nf, Nt, (flags & FDR_ZDT_MIXED_PRECISION) != 0, &pl, &ql);
+  fused_split_log2(Nf, Nt, &pl, &ql);
   *P = (int64_t)1 << pl;
   *Q = (int64_t)1 << ql;
   return FDR_OK;

@@ -35,6 +35,7 @@
 
 #include "fft_device.cuh"
 #include "fft_engine.cuh"
+#include "umma.cuh"
 #include "zdt_ws.cuh"
 
 namespace cg = cooperative_groups;
@@ -2099,6 +2100,310 @@ zdtf_output_mma_kernel(const __grid_constant__ CUtensorMap wmap, long long N, in
 }
 
 // ------------------------------------------------------------------------------------
+// Mixed-precision output pass for P = 2048 = 32 x 64 on the fifth-generation tensor cores
+// (tcgen05, accumulators in tensor memory).  Per tile (rate pair q, 8 residues) the inverse
+// DFT_P of sequence s,
+//   z[s][n + 32 c] = sum_r e^(2 pi i r c / 64) e^(2 pi i r n / 2048) sum_m e^(2 pi i m n / 32) x[s][r + 64 m],
+// runs as two real-embedded contractions with bfloat16 split operands (v = hi + lo, hi =
+// bf16(v), lo = bf16(v - hi); hi*hi + hi*lo + lo*hi accumulated in float32, the lo*lo term,
+// ~2^-16 relative, dropped):
+//   pass 1: D1 (512 x 64)  = X (512 x 64) * E32 (64 x 64)    rows (s, r), K (m, re/im), N (n, re/im)
+//   pass 2: D2 (128 x 256) = E64 (128 x 128) * Y (128 x 256) rows (re/im, c), K (re/im, r), N (s, n)
+// X is the W tile (TMA, 128 KB) converted in place to a K-major operand; Y is pass 1's output
+// times the inter-pass twiddle, which the pass-1 epilogue writes into the same region as an
+// MN-major operand, so no transpose is needed between the passes.  Pass 2's rows are the
+// pair's two rates (real parts: rate j, imaginary parts: rate j + 1); each epilogue thread
+// holds 8 residues of one rate per output channel and stores them as two 16-byte vectors.
+// The next tile's fetch is issued once pass 2's MMAs have read Y, so it overlaps the FDR
+// stores.  Every mbarrier wait is bounded (kTmaWaitNs); tensor memory is freed on all paths.
+// ------------------------------------------------------------------------------------
+struct OutUmmaShape {
+  static constexpr int P = 2048, P1 = 64, P2 = 32, TS = 8, T = 512;
+  static constexpr unsigned TILEB = sizeof(float2) * P * TS;  // 128 KB
+  static constexpr int BOXR = 256, NBOX = P / BOXR;
+  // byte layouts of the operands (core matrices of 8 rows x 16 bytes; umma.cuh)
+  static constexpr unsigned X_SBO = 1024, X_LBO = 128, X_PART = 65536;  // K-major; hi, then lo
+  static constexpr unsigned E32_SBO = 1024, E32_LBO = 128, E32_PART = 8192;
+  static constexpr unsigned E64_SBO = 2048, E64_LBO = 128, E64_PART = 32768;
+  static constexpr unsigned Y_SBO = 128, Y_LBO = 4096, Y_PART = 65536;  // MN-major
+  static constexpr int S1 = P2 + 1;  // twiddle table rows
+  static constexpr unsigned OFF_E32 = TILEB;
+  static constexpr unsigned OFF_E64 = OFF_E32 + 2 * E32_PART;
+  static constexpr unsigned OFF_TW = OFF_E64 + 2 * E64_PART;
+  static constexpr unsigned OFF_BAR = OFF_TW + sizeof(float2) * P1 * S1;
+  static constexpr size_t SMEM = 1024 + OFF_BAR + 32;
+  static constexpr unsigned TMEM_COLS = 256;  // D1 (4 blocks x 64 columns), then D2 (256)
+};
+static_assert(OutUmmaShape::SMEM <= 232448, "zdtf_output_umma_kernel: shared memory");
+static_assert(OutUmmaShape::OFF_BAR % 8 == 0, "zdtf_output_umma_kernel: mbarrier alignment");
+
+// Row of X (and lane of D1) of sequence (s, r).  16-byte shared-memory accesses are served
+// per 8 lanes, which must hit 8 different 16-byte bank slots: the 8 converting lanes of one
+// r (s = lane mod 8) write rows with 8 different (row mod 8), and the 8 epilogue lanes of
+// one 8-row group (row = thread) hold 8 different r mod 8, i.e. the 8 K rows of one core
+// matrix of Y.
+__device__ __forceinline__ int umma_xrow(int s, int r) {
+  return ((r + s) & 7) + 8 * s + 64 * (r >> 3);
+}
+// Byte offset of element (row, k) of a K-major operand (K chunks 128 bytes apart).
+__device__ __forceinline__ unsigned umma_kmaj(int row, int k, unsigned sbo) {
+  return (unsigned)(row >> 3) * sbo + (unsigned)(k >> 3) * 128u + (unsigned)(row & 7) * 16u +
+         (unsigned)(k & 7) * 2u;
+}
+// a = hi + lo, b = hi' + lo' in bfloat16, packed two per word (a in the low half).
+__device__ __forceinline__ void umma_split2(float a, float b, unsigned& hi, unsigned& lo) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+  const float2 hf = __bfloat1622float2(h);
+  const __nv_bfloat162 l = __floats2bfloat162_rn(a - hf.x, b - hf.y);
+  hi = *reinterpret_cast<const unsigned*>(&h);
+  lo = *reinterpret_cast<const unsigned*>(&l);
+}
+
+__global__ void __launch_bounds__(OutUmmaShape::T, 1)
+zdtf_output_umma_kernel(const __grid_constant__ CUtensorMap wmap, long long N, int Q, int Nr,
+                        int npairs, float* __restrict__ dest, const float2* __restrict__ rootsP,
+                        double* __restrict__ acc) {
+  using SH = OutUmmaShape;
+  constexpr int P = SH::P, P1 = SH::P1, P2 = SH::P2, TS = SH::TS;
+  extern __shared__ unsigned char smraw[];
+  unsigned char* sm = (unsigned char*)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
+  float2* region = (float2*)sm;
+  unsigned char* e32 = sm + SH::OFF_E32;
+  unsigned char* e64 = sm + SH::OFF_E64;
+  float2* tw = (float2*)(sm + SH::OFF_TW);
+  unsigned long long* bar = (unsigned long long*)(sm + SH::OFF_BAR);  // [0] TMA, [1] MMA
+  unsigned* tslot = (unsigned*)(bar + 2);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int ntna = Q / TS;
+  const long long ntiles = (long long)ntna * npairs;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    umma::tmem_alloc(tslot, SH::TMEM_COLS);
+    umma::tmem_relinquish();
+  }
+  // E32 (B of pass 1, K-major): row nu = 2 n + re/im of the output, K pair (Re, Im) of x_m
+  for (int e = tid; e < 64 * 32; e += SH::T) {
+    const int nu = e >> 5, m = e & 31, n = nu >> 1, co = nu & 1;
+    const float2 w = cconj(__ldg(rootsP + ((64 * m * n) & (P - 1))));  // e^(2 pi i m n / 32)
+    unsigned h, l;
+    umma_split2(co ? w.y : w.x, co ? w.x : -w.y, h, l);
+    const unsigned off = umma_kmaj(nu, 2 * m, SH::E32_SBO);
+    *reinterpret_cast<unsigned*>(e32 + off) = h;
+    *reinterpret_cast<unsigned*>(e32 + SH::E32_PART + off) = l;
+  }
+  // E64 (A of pass 2, K-major): row 64 re/im + c, K 64 re/im + r, pairs (r, r + 1)
+  for (int e = tid; e < 128 * 64; e += SH::T) {
+    const int row = e >> 6, k0 = 2 * (e & 63);
+    const int co = row >> 6, c = row & 63, ci = k0 >> 6, r0 = k0 & 63;
+    float v[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const float2 w = cconj(__ldg(rootsP + ((32 * (r0 + u) * c) & (P - 1))));  // e^(2 pi i r c / 64)
+      v[u] = co == ci ? w.x : (co == 0 ? -w.y : w.y);
+    }
+    unsigned h, l;
+    umma_split2(v[0], v[1], h, l);
+    const unsigned off = umma_kmaj(row, k0, SH::E64_SBO);
+    *reinterpret_cast<unsigned*>(e64 + off) = h;
+    *reinterpret_cast<unsigned*>(e64 + SH::E64_PART + off) = l;
+  }
+  for (int i = tid; i < P1 * P2; i += SH::T)
+    tw[(i / P2) * SH::S1 + i % P2] = cconj(__ldg(rootsP + (((i / P2) * (i % P2)) & (P - 1))));
+  umma::fence_smem_to_async();
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const unsigned tbase = *tslot;
+  const unsigned sb = umma::smem_u32(sm);
+  auto issue = [&](long long tile) {  // thread 0 only
+    const int q = (int)(tile / ntna), nat = (int)(tile - (long long)q * ntna);
+    mbar_expect_tx(&bar[0], SH::TILEB);
+#pragma unroll
+    for (int b = 0; b < SH::NBOX; ++b)
+      tma_load_2d(region + b * SH::BOXR * TS, &wmap, 2 * TS * nat, q * P + b * SH::BOXR, &bar[0]);
+  };
+  const long long first = blockIdx.x, stride = gridDim.x;
+  if (tid == 0 && first < ntiles) issue(first);
+  constexpr unsigned idesc1 = umma::idesc_bf16_f32(128, 64, false, false);
+  constexpr unsigned idesc2 = umma::idesc_bf16_f32(128, 256, false, true);
+  const int cs = tid & 7, cr = tid >> 3;  // converting role: sequence (s, r)
+  const int crow = umma_xrow(cs, cr);
+  const int es = (tid >> 3) & 7;  // pass-1 epilogue role: row tid of D1
+  const int er = (((tid & 7) - es) & 7) + 8 * (tid >> 6);
+  const unsigned lane_base = (unsigned)(32 * (warp & 3)) << 16;
+  unsigned mph = 0;
+  bool fail = false, mma_out = false;
+  int it = 0;
+  for (long long tile = first; tile < ntiles; tile += stride, ++it) {
+    const bool ok = mbar_wait_bounded(&bar[0], (unsigned)(it & 1));
+    if (__syncthreads_or(!ok)) { fail = true; break; }
+    const int q = (int)(tile / ntna), nat = (int)(tile - (long long)q * ntna);
+    const int na0 = nat * TS;
+    {  // the W tile to registers, then in place to X (hi, lo)
+      float2 v[P2];
+#pragma unroll
+      for (int m = 0; m < P2; ++m) v[m] = region[(cr + P1 * m) * TS + cs];
+      __syncthreads();
+      unsigned char* xr = sm + (unsigned)(crow >> 3) * SH::X_SBO + (unsigned)(crow & 7) * 16u;
+#pragma unroll
+      for (int kc = 0; kc < 8; ++kc) {  // K chunk kc: x_m for m = 4 kc .. 4 kc + 3
+        uint4 h, l;
+        umma_split2(v[4 * kc].x, v[4 * kc].y, h.x, l.x);
+        umma_split2(v[4 * kc + 1].x, v[4 * kc + 1].y, h.y, l.y);
+        umma_split2(v[4 * kc + 2].x, v[4 * kc + 2].y, h.z, l.z);
+        umma_split2(v[4 * kc + 3].x, v[4 * kc + 3].y, h.w, l.w);
+        *reinterpret_cast<uint4*>(xr + kc * 128) = h;
+        *reinterpret_cast<uint4*>(xr + SH::X_PART + kc * 128) = l;
+      }
+    }
+    umma::fence_smem_to_async();
+    umma::fence_before_sync();
+    __syncthreads();
+    if (tid == 0) {  // pass 1: 4 row blocks x 4 K steps x 3 products
+      umma::fence_after_sync();
+#pragma unroll 1
+      for (int b = 0; b < 4; ++b) {
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          const unsigned xa = sb + (unsigned)b * 16u * SH::X_SBO + (unsigned)t * 256u;
+          const unsigned ea = sb + SH::OFF_E32 + (unsigned)t * 256u;
+          const uint64_t xh = umma::sdesc(xa, SH::X_LBO, SH::X_SBO);
+          const uint64_t xl = umma::sdesc(xa + SH::X_PART, SH::X_LBO, SH::X_SBO);
+          const uint64_t eh = umma::sdesc(ea, SH::E32_LBO, SH::E32_SBO);
+          const uint64_t el = umma::sdesc(ea + SH::E32_PART, SH::E32_LBO, SH::E32_SBO);
+          umma::mma_bf16(tbase + 64u * b, xh, eh, idesc1, t > 0);
+          umma::mma_bf16(tbase + 64u * b, xh, el, idesc1, true);
+          umma::mma_bf16(tbase + 64u * b, xl, eh, idesc1, true);
+        }
+      }
+      umma::commit(&bar[1]);
+    }
+    bool okm = mbar_wait_bounded(&bar[1], mph);
+    mph ^= 1u;
+    if (__syncthreads_or(!okm)) { fail = mma_out = true; break; }
+    umma::fence_after_sync();
+    {  // pass-1 epilogue: row tid of D1 times the twiddle, to Y (hi, lo)
+      float d[64];
+      umma::ld64_wait(tbase + lane_base + 64u * (unsigned)(tid >> 7), d);
+      const float2* twr = tw + er * SH::S1;
+      unsigned char* yre = sm + (unsigned)(er >> 3) * SH::Y_LBO + (unsigned)(er & 7) * 16u;
+      unsigned char* yim = yre + 8u * SH::Y_LBO;  // K row 64 + er
+#pragma unroll
+      for (int g = 0; g < 4; ++g) {  // channels n = 8 g .. 8 g + 7
+        unsigned rh[4], rl[4], ih[4], il[4];
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+          const int n0 = 8 * g + 2 * p;
+          const float2 y0 = cmul(make_float2(d[2 * n0], d[2 * n0 + 1]), twr[n0]);
+          const float2 y1 = cmul(make_float2(d[2 * n0 + 2], d[2 * n0 + 3]), twr[n0 + 1]);
+          umma_split2(y0.x, y1.x, rh[p], rl[p]);
+          umma_split2(y0.y, y1.y, ih[p], il[p]);
+        }
+        const unsigned nofs = (unsigned)(4 * es + g) * SH::Y_SBO;  // N group (32 es + 8 g) / 8
+        *reinterpret_cast<uint4*>(yre + nofs) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
+        *reinterpret_cast<uint4*>(yre + SH::Y_PART + nofs) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
+        *reinterpret_cast<uint4*>(yim + nofs) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
+        *reinterpret_cast<uint4*>(yim + SH::Y_PART + nofs) = make_uint4(il[0], il[1], il[2], il[3]);
+      }
+    }
+    umma::fence_smem_to_async();
+    umma::fence_before_sync();
+    __syncthreads();
+    if (tid == 0) {  // pass 2: 8 K steps x 3 products into columns 0..255
+      umma::fence_after_sync();
+#pragma unroll
+      for (int t = 0; t < 8; ++t) {
+        const unsigned ea = sb + SH::OFF_E64 + (unsigned)t * 256u;
+        const unsigned ya = sb + (unsigned)(2 * t) * SH::Y_LBO;
+        const uint64_t eh = umma::sdesc(ea, SH::E64_LBO, SH::E64_SBO);
+        const uint64_t el = umma::sdesc(ea + SH::E64_PART, SH::E64_LBO, SH::E64_SBO);
+        const uint64_t yh = umma::sdesc(ya, SH::Y_LBO, SH::Y_SBO);
+        const uint64_t yl = umma::sdesc(ya + SH::Y_PART, SH::Y_LBO, SH::Y_SBO);
+        umma::mma_bf16(tbase, eh, yh, idesc2, t > 0);
+        umma::mma_bf16(tbase, eh, yl, idesc2, true);
+        umma::mma_bf16(tbase, el, yh, idesc2, true);
+      }
+      umma::commit(&bar[1]);
+    }
+    okm = mbar_wait_bounded(&bar[1], mph);
+    mph ^= 1u;
+    if (__syncthreads_or(!okm)) { fail = mma_out = true; break; }
+    umma::fence_after_sync();
+    if (tid == 0 && tile + stride < ntiles) {  // Y is read: refill the region
+      umma::fence_smem_to_async();
+      issue(tile + stride);
+    }
+    {  // pass-2 epilogue: lane (re/im, c) of D2, channels n = 8 (warp / 4) .. + 7, 8 residues
+      const int co = (warp & 3) >> 1, c = 32 * (warp & 1) + lane, ng = warp >> 2;
+      const int j = 2 * q;
+      float z[64];  // z[8 s + i]: channel 8 ng + i of residue s
+      umma::ld8x8_wait<32>(tbase + lane_base + 8u * (unsigned)ng, z);
+      if (co == 0 || j + 1 < Nr) {
+        // The 8 residues of one (rate, channel) are one 32-byte sector.  Lanes 2k and 2k + 1
+        // (channels c, c + 1) write both halves of one sector per instruction: the even
+        // lane passes residues 4-7 of its channel to the odd lane, the odd lane residues
+        // 0-3 of its channel to the even lane, so each store instruction fills 16 sectors.
+        const bool odd = lane & 1;
+        float* col = dest + (long long)(j + co) * N + na0;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const float4 lo = make_float4(z[i], z[8 + i], z[16 + i], z[24 + i]);
+          const float4 hi = make_float4(z[32 + i], z[40 + i], z[48 + i], z[56 + i]);
+          const float4 snd = odd ? lo : hi;
+          float4 rcv;
+          rcv.x = __shfl_xor_sync(0xffffffffu, snd.x, 1);
+          rcv.y = __shfl_xor_sync(0xffffffffu, snd.y, 1);
+          rcv.z = __shfl_xor_sync(0xffffffffu, snd.z, 1);
+          rcv.w = __shfl_xor_sync(0xffffffffu, snd.w, 1);
+          float* pe = col + (long long)Q * (8 * ng + i + 32 * (c & ~1));  // even channel's sector
+          float* po = pe + (long long)Q * 32;                             // odd channel's sector
+          float* da = odd ? pe + 4 : pe;
+          float* db = odd ? po + 4 : po;
+          if (FDR_DBG_OK(da >= dest && da + 4 <= dest + N * (long long)Nr))
+            __stcs(reinterpret_cast<float4*>(da), odd ? rcv : lo);
+          if (FDR_DBG_OK(db >= dest && db + 4 <= dest + N * (long long)Nr))
+            __stcs(reinterpret_cast<float4*>(db), odd ? hi : rcv);
+        }
+        if (acc) {
+          double s1 = 0.0, s2 = 0.0;
+#pragma unroll
+          for (int e = 0; e < 64; ++e) {
+            const double x = z[e];
+            s1 += x;
+            s2 += x * x;
+          }
+          for (int o = 16; o > 0; o >>= 1) {
+            s1 += __shfl_down_sync(0xffffffffu, s1, o);
+            s2 += __shfl_down_sync(0xffffffffu, s2, o);
+          }
+          if (lane == 0) {
+            atomicAdd(acc + 2 * (j + co), s1);
+            atomicAdd(acc + 2 * (j + co) + 1, s2);
+          }
+        }
+      }
+    }
+    umma::fence_before_sync();
+  }
+  if (fail) {
+    if (tid == 0) atomicOr(&g_fused_fault, 16);
+    // an MMA group whose wait ran out may still be running: give it one more bounded wait
+    // before its tensor memory is freed
+    if (mma_out) (void)mbar_wait_bounded(&bar[1], mph ^ 1u);
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    umma::fence_after_sync();
+    umma::tmem_dealloc(tbase, SH::TMEM_COLS);
+  }
+}
+
+// ------------------------------------------------------------------------------------
 // Host side
 // ------------------------------------------------------------------------------------
 // Tile (sequences per CTA) and block size of kernels A and C for a given P: one radix-16
@@ -2120,20 +2425,19 @@ struct CztShape {  // buf | twt | twr | gnyq | buf2 (the second rate-block buffe
 // log2 of the four-step factor Q for Nf = 2^L and Nt time steps.  With F in registers
 // (Nt <= 16): 512 bins per CTA up to Nf = 2^20 (256 threads, two CTAs per SM, so one CTA's
 // barriers overlap the other's Horner sums; P <= 2048 keeps the TMA output passes), 1024
-// above; with F in shared memory 512 (Nt <= 32) and 256 (Nt <= 64).  p1024 (the
-// mixed-precision output pass, whose tensor-core DFTs are written for P = 1024) keeps 1024
-// bins per CTA for Nt <= 16, so that Nf = 2^20 splits as 1024 x 1024.
-static int fused_qlog(int L, int64_t Nt, bool p1024 = false) {
+// above; with F in shared memory 512 (Nt <= 32) and 256 (Nt <= 64).  Mixed-precision
+// workspaces split the same way (their tensor-core output passes cover P = 1024 and 2048).
+static int fused_qlog(int L, int64_t Nt) {
   // 32 < Nt <= 64 at Nf = 2^20, 2^21: 512 bins per residue pair, F split over a cluster of two
   // CTAs (zdtf_czt_cl_kernel), so that P stays 2048 / 4096
-  const int cap = Nt <= 16 ? ((L <= 20 && !p1024) ? 9 : 10)
+  const int cap = Nt <= 16 ? (L <= 20 ? 9 : 10)
                            : (Nt <= 32 ? 9 : ((L == 20 || L == 21) ? 9 : 8));
   return std::min(cap, (L + 1) / 2);
 }
 
-void fused_split_log2(int64_t Nf, int64_t Nt, bool p1024, int* Plog, int* Qlog) {
+void fused_split_log2(int64_t Nf, int64_t Nt, int* Plog, int* Qlog) {
   const int L = ilog2(Nf);
-  *Qlog = fused_qlog(L, Nt, p1024);
+  *Qlog = fused_qlog(L, Nt);
   *Plog = L - *Qlog;
 }
 
@@ -2245,6 +2549,8 @@ static int set_smem_attrs() {
 #undef SET_C2
   FDR_CUDA(cudaFuncSetAttribute(zdtf_output_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)OutMmaShape::SMEM));
+  FDR_CUDA(cudaFuncSetAttribute(zdtf_output_umma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)OutUmmaShape::SMEM));
   FDR_CUDA(cudaFuncSetAttribute(zdtf_output_tma_kernel<32, 32, 8>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)OutTmaShape<32, 32, 8>::SMEM));
@@ -2286,7 +2592,7 @@ static int set_smem_attrs() {
   return FDR_OK;
 }
 
-int fused_plan_create(FusedPlan** out, int64_t N, int64_t Nt, int64_t Nr, bool p1024) {
+int fused_plan_create(FusedPlan** out, int64_t N, int64_t Nt, int64_t Nr) {
   *out = nullptr;
   if (!zdt_fused_eligible(N, Nt, Nr)) {
     set_error(FDR_ERR_UNSUPPORTED_SIZE, "fused plan: Nf=%lld Nt=%lld not supported",
@@ -2297,7 +2603,7 @@ int fused_plan_create(FusedPlan** out, int64_t N, int64_t Nt, int64_t Nr, bool p
   FusedPlan* st = new FusedPlan();
   st->N = N; st->Nt = Nt; st->Nr = Nr;
   st->L = ilog2(N);
-  const int Qlog = fused_qlog(st->L, Nt, p1024);
+  const int Qlog = fused_qlog(st->L, Nt);
   st->Q = 1 << Qlog;
   st->P = (int)(N >> Qlog);
   st->B = (st->L + 1) / 2;
@@ -2553,9 +2859,22 @@ int fused_take_fault() {
   return FDR_OK;
 }
 
-// The output pass with the split-bfloat16 tensor-core DFTs (P = 1024 only; other shapes and a
-// failed tensor-map encode use the float32 kernels).
+// The output pass with the split-bfloat16 tensor-core DFTs: tcgen05 for P = 2048, mma.sync
+// for P = 1024 (other shapes, an unaligned destination and a failed tensor-map encode use
+// the float32 kernels).
 int fused_output_mixed(const FusedPlan* st, const float2* W, float* dest, double* acc, cudaStream_t s) {
+  if (st->P == 2048 && st->Q >= 8 && ((uintptr_t)dest & 15) == 0) {
+    CUtensorMap map;
+    using SH = OutUmmaShape;
+    if (w_tensor_map(&map, W, st->Q, st->npairs * (int64_t)st->P, SH::TS)) {
+      const long long ntiles = (long long)(st->Q / SH::TS) * st->npairs;
+      const int grid = (int)std::min<long long>(ntiles, sm_count());
+      zdtf_output_umma_kernel<<<grid, SH::T, SH::SMEM, s>>>(
+          map, st->N, st->Q, (int)st->Nr, (int)st->npairs, dest, st->tab.rootsP, acc);
+      FDR_LAUNCH_CHECK("zdtf_output_umma_kernel");
+      return FDR_OK;
+    }
+  }
   if (st->P == 1024 && st->Q >= 8) {
     CUtensorMap map;
     if (w_tensor_map(&map, W, st->Q, st->npairs * (int64_t)st->P, 8)) {
@@ -2629,7 +2948,7 @@ static FusedPlan* st_of(fdr_zdt* ws) { return reinterpret_cast<FusedPlan*>(ws->f
 
 int zdt_fused_setup(fdr_zdt* ws) {
   FusedPlan* st = nullptr;
-  FDR_TRY(fused_plan_create(&st, ws->Nf, ws->Nt, ws->Nr, (ws->flags & FDR_ZDT_MIXED_PRECISION) != 0));
+  FDR_TRY(fused_plan_create(&st, ws->Nf, ws->Nt, ws->Nr));
   ws->fstate = st;
   ws->fP = st->P;
   ws->fQ = st->Q;

@@ -44,7 +44,7 @@ int zdt_ensure_F(fdr_zdt* ws, cudaStream_t s);
 // Fused path (zdt_fused.cu)
 bool zdt_fused_eligible(int64_t Nf, int64_t Nt, int64_t Nr);
 // log2 of P and Q of the fused split (Nf a power of two, zdt_fused_eligible true).
-void fused_split_log2(int64_t Nf, int64_t Nt, bool p1024, int* Plog, int* Qlog);
+void fused_split_log2(int64_t Nf, int64_t Nt, int* Plog, int* Qlog);
 int zdt_fused_setup(fdr_zdt* ws);
 int zdt_fused_input(fdr_zdt* ws, const float* spec, cudaStream_t s);
 int zdt_fused_A_to_F(fdr_zdt* ws, cudaStream_t s);
@@ -58,7 +58,7 @@ void zdt_fused_release(fdr_zdt* ws);
 
 // Fused kernels for one (Nf, Nt, Nr) shape with caller-owned intermediates (zdt_fused.cu).
 struct FusedPlan;
-int fused_plan_create(FusedPlan** out, int64_t N, int64_t Nt, int64_t Nr, bool p1024 = false);
+int fused_plan_create(FusedPlan** out, int64_t N, int64_t Nt, int64_t Nr);
 void fused_plan_destroy(FusedPlan* st);
 int64_t fused_plan_table_bytes(const FusedPlan* st);
 int64_t fused_A_elems(const FusedPlan* st);

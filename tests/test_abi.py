@@ -60,13 +60,14 @@ def test_argument_errors_without_device(fdr):
 
 def test_fused_split_plan(fdr):
     """The four-step split of the fused path, chosen on the host: 512 bins per czt CTA up to
-    Nf = 2^20 with F in registers (Nt <= 16), 1024 above and for mixed-precision workspaces
-    at 2^20 (their tensor-core output pass is written for P = 1024), 512 / 256 bins with F
+    Nf = 2^20 with F in registers (Nt <= 16), 1024 above (mixed-precision workspaces split
+    the same way: their tensor-core output passes cover P = 1024 and 2048), 512 / 256 bins with F
     in shared memory (Nt <= 32 / 64), and 512 bins at Nf = 2^20 and 2^21 for 32 < Nt <= 64
     (F split over a two-CTA cluster); the staged kernels outside 2^12..2^22 or P > 4096."""
     fs = fdr.fused_split
     assert fs(2 ** 20, 16, 129) == (2048, 512)
-    assert fs(2 ** 20, 16, 129, mixed_precision=True) == (1024, 1024)
+    assert fs(2 ** 20, 16, 129, mixed_precision=True) == (2048, 512)
+    assert fs(2 ** 19, 16, 129, mixed_precision=True) == (1024, 512)
     assert fs(2 ** 19, 16, 129) == (1024, 512)
     assert fs(2 ** 21, 16, 17) == (2048, 1024)
     assert fs(2 ** 22, 16, 17) == (4096, 1024)
