@@ -13,7 +13,8 @@ pytestmark = pytest.mark.gpu
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 SUITES = ["tests/test_gpu_fused.py", "tests/test_gpu_intfdr.py", "tests/test_gpu_fdrutils.py",
-          "tests/test_gpu_random_shapes.py", "tests/test_gpu_h5ingest.py", "tests/test_gpu_zdt.py"]
+          "tests/test_gpu_random_shapes.py", "tests/test_gpu_h5ingest.py", "tests/test_gpu_zdt.py",
+          "tests/test_gpu_mixed.py"]
 
 
 def test_debug_build_runs_the_parity_suites_without_violations():
