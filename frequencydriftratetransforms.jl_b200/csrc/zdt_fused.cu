@@ -1579,6 +1579,15 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
       : "memory");
 }
 
+// 3-D tiled TMA load (no multicast) of box {x .. x+15 floats, y .. y+31, z .. z+31} into dst.
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z,
+                                            unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+      ::"r"(smem_addr(dst)), "l"((unsigned long long)map), "r"(x), "r"(y), "r"(z), "r"(smem_addr(bar))
+      : "memory");
+}
+
 // The W tile lands (TMA) in a region that pass 1 then overwrites with its transposed
 // output, so a CTA needs ~76 KB and two fit per SM; the next tile's fetch is issued as soon
 // as pass 2 has read the region, overlapping pass 2's DFTs and FDR stores (and the other
@@ -2108,40 +2117,44 @@ zdtf_output_mma_kernel(const __grid_constant__ CUtensorMap wmap, long long N, in
 // bf16(v), lo = bf16(v - hi); hi*hi + hi*lo + lo*hi accumulated in float32, the lo*lo term,
 // ~2^-16 relative, dropped):
 //   pass 1: D1 (512 x 64)  = X (512 x 64) * E32 (64 x 64)    rows (s, r), K (m, re/im), N (n, re/im)
-//   pass 2: D2 (128 x 256) = E64 (128 x 128) * Y (128 x 256) rows (re/im, c), K (re/im, r), N (s, n)
-// X is the W tile (TMA, 128 KB) converted in place to a K-major operand; Y is pass 1's output
-// times the inter-pass twiddle, which the pass-1 epilogue writes into the same region as an
-// MN-major operand, so no transpose is needed between the passes.  Pass 2's rows are the
-// pair's two rates (real parts: rate j, imaginary parts: rate j + 1); each epilogue thread
-// holds 8 residues of one rate per output channel and stores them as two 16-byte vectors.
-// The next tile's fetch is issued once pass 2's MMAs have read Y, so it overlaps the FDR
-// stores.  Every mbarrier wait is bounded (kTmaWaitNs); tensor memory is freed on all paths.
+//   pass 2: D2 (128 x 256) = E64 (128 x 128) * Y (128 x 256) rows (re/im, c), K (r, re/im), N (s, n)
+// The tile is fetched (TMA, 3-D tensor map) as two 64 KB halves, r < 32 and r >= 32, and
+// processed as a pipeline over the halves: half h is converted in place to its 256 rows of
+// X (K-major) while the MMAs of the other half run; pass 1's epilogue for half h writes, in
+// place again, the 64 K rows of Y (MN-major, no transpose between the passes) that pass 2
+// consumes as its K steps 4h .. 4h + 3; and half h is refilled with the next tile as soon as
+// those MMAs have read it, so the fetch overlaps the rest of the tile and the FDR stores.
+// Pass 2's rows are the pair's two rates (real parts: rate j, imaginary parts: rate j + 1);
+// each epilogue lane holds 8 residues of one rate per output channel, and lane pairs store
+// whole 32-byte sectors.  Every mbarrier wait is bounded (kTmaWaitNs); tensor memory is
+// freed on all paths.
 // ------------------------------------------------------------------------------------
 struct OutUmmaShape {
   static constexpr int P = 2048, P1 = 64, P2 = 32, TS = 8, T = 512;
-  static constexpr unsigned TILEB = sizeof(float2) * P * TS;  // 128 KB
-  static constexpr int BOXR = 256, NBOX = P / BOXR;
-  // byte layouts of the operands (core matrices of 8 rows x 16 bytes; umma.cuh)
-  static constexpr unsigned X_SBO = 1024, X_LBO = 128, X_PART = 65536;  // K-major; hi, then lo
+  static constexpr unsigned HALF = 65536;  // one half tile: 8 residues x 32 r x 32 m
+  // byte layouts of the operands (core matrices of 8 rows x 16 bytes; umma.cuh); X and Y
+  // of half h live in region half h, hi then lo
+  static constexpr unsigned X_SBO = 1024, X_LBO = 128, X_PART = 32768;  // K-major, 256 rows
+  static constexpr unsigned Y_SBO = 128, Y_LBO = 4096, Y_PART = 32768;  // MN-major, 64 K rows
   static constexpr unsigned E32_SBO = 1024, E32_LBO = 128, E32_PART = 8192;
   static constexpr unsigned E64_SBO = 2048, E64_LBO = 128, E64_PART = 32768;
-  static constexpr unsigned Y_SBO = 128, Y_LBO = 4096, Y_PART = 65536;  // MN-major
   static constexpr int S1 = P2 + 1;  // twiddle table rows
-  static constexpr unsigned OFF_E32 = TILEB;
+  static constexpr unsigned OFF_E32 = 2 * HALF;
   static constexpr unsigned OFF_E64 = OFF_E32 + 2 * E32_PART;
   static constexpr unsigned OFF_TW = OFF_E64 + 2 * E64_PART;
   static constexpr unsigned OFF_BAR = OFF_TW + sizeof(float2) * P1 * S1;
-  static constexpr size_t SMEM = 1024 + OFF_BAR + 32;
-  static constexpr unsigned TMEM_COLS = 256;  // D1 (4 blocks x 64 columns), then D2 (256)
+  static constexpr size_t SMEM = 1024 + OFF_BAR + 64;
+  static constexpr unsigned TMEM_COLS = 512;  // D1: 4 blocks x 64 columns; D2: 256 columns
+  static constexpr unsigned D2_COL = 256;
 };
 static_assert(OutUmmaShape::SMEM <= 232448, "zdtf_output_umma_kernel: shared memory");
 static_assert(OutUmmaShape::OFF_BAR % 8 == 0, "zdtf_output_umma_kernel: mbarrier alignment");
 
-// Row of X (and lane of D1) of sequence (s, r).  16-byte shared-memory accesses are served
-// per 8 lanes, which must hit 8 different 16-byte bank slots: the 8 converting lanes of one
-// r (s = lane mod 8) write rows with 8 different (row mod 8), and the 8 epilogue lanes of
-// one 8-row group (row = thread) hold 8 different r mod 8, i.e. the 8 K rows of one core
-// matrix of Y.
+// Row of X (and lane of D1) of sequence (s, r); block r / 16, so half h holds rows
+// 256 h .. 256 h + 255.  16-byte shared-memory accesses are served per 8 lanes, which must
+// hit 8 different 16-byte bank slots: the 8 converting lanes of one r (s = lane mod 8)
+// write rows with 8 different (row mod 8), and the 8 epilogue lanes of one 8-row group
+// hold 8 different r mod 8, i.e. the 8 K rows of one core matrix of Y.
 __device__ __forceinline__ int umma_xrow(int s, int r) {
   return ((r + s) & 7) + 8 * s + 64 * (r >> 3);
 }
@@ -2167,18 +2180,18 @@ zdtf_output_umma_kernel(const __grid_constant__ CUtensorMap wmap, long long N, i
   constexpr int P = SH::P, P1 = SH::P1, P2 = SH::P2, TS = SH::TS;
   extern __shared__ unsigned char smraw[];
   unsigned char* sm = (unsigned char*)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
-  float2* region = (float2*)sm;
   unsigned char* e32 = sm + SH::OFF_E32;
   unsigned char* e64 = sm + SH::OFF_E64;
   float2* tw = (float2*)(sm + SH::OFF_TW);
-  unsigned long long* bar = (unsigned long long*)(sm + SH::OFF_BAR);  // [0] TMA, [1] MMA
-  unsigned* tslot = (unsigned*)(bar + 2);
+  // mbarriers: [0], [1] the two halves' fetches; [2], [3] pass 1 of half 0, 1; [4], [5]
+  // pass 2's K steps of half 0, 1.  Each completes once per tile.
+  unsigned long long* bar = (unsigned long long*)(sm + SH::OFF_BAR);
+  unsigned* tslot = (unsigned*)(bar + 6);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int ntna = Q / TS;
   const long long ntiles = (long long)ntna * npairs;
   if (tid == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
+    for (int i = 0; i < 6; ++i) mbar_init(&bar[i], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
@@ -2195,10 +2208,11 @@ zdtf_output_umma_kernel(const __grid_constant__ CUtensorMap wmap, long long N, i
     *reinterpret_cast<unsigned*>(e32 + off) = h;
     *reinterpret_cast<unsigned*>(e32 + SH::E32_PART + off) = l;
   }
-  // E64 (A of pass 2, K-major): row 64 re/im + c, K 64 re/im + r, pairs (r, r + 1)
+  // E64 (A of pass 2, K-major): row 64 re/im + c; K 64 h + 32 re/im + (r mod 32) for
+  // r = 32 h + (r mod 32), so that K steps 4h .. 4h + 3 are half h's; pairs (r, r + 1)
   for (int e = tid; e < 128 * 64; e += SH::T) {
     const int row = e >> 6, k0 = 2 * (e & 63);
-    const int co = row >> 6, c = row & 63, ci = k0 >> 6, r0 = k0 & 63;
+    const int co = row >> 6, c = row & 63, ci = (k0 >> 5) & 1, r0 = 32 * (k0 >> 6) + (k0 & 31);
     float v[2];
 #pragma unroll
     for (int u = 0; u < 2; ++u) {
@@ -2219,129 +2233,164 @@ zdtf_output_umma_kernel(const __grid_constant__ CUtensorMap wmap, long long N, i
   umma::fence_after_sync();
   const unsigned tbase = *tslot;
   const unsigned sb = umma::smem_u32(sm);
-  auto issue = [&](long long tile) {  // thread 0 only
+  auto issue = [&](long long tile, int h) {  // thread 0 only: half h of a tile
     const int q = (int)(tile / ntna), nat = (int)(tile - (long long)q * ntna);
-    mbar_expect_tx(&bar[0], SH::TILEB);
-#pragma unroll
-    for (int b = 0; b < SH::NBOX; ++b)
-      tma_load_2d(region + b * SH::BOXR * TS, &wmap, 2 * TS * nat, q * P + b * SH::BOXR, &bar[0]);
+    mbar_expect_tx(&bar[h], SH::HALF);
+    tma_load_3d(sm + h * SH::HALF, &wmap, 2 * TS * nat, 32 * h, 32 * q, &bar[h]);
   };
   const long long first = blockIdx.x, stride = gridDim.x;
-  if (tid == 0 && first < ntiles) issue(first);
+  if (tid == 0 && first < ntiles) {
+    issue(first, 0);
+    issue(first, 1);
+  }
   constexpr unsigned idesc1 = umma::idesc_bf16_f32(128, 64, false, false);
   constexpr unsigned idesc2 = umma::idesc_bf16_f32(128, 256, false, true);
-  const int cs = tid & 7, cr = tid >> 3;  // converting role: sequence (s, r)
-  const int crow = umma_xrow(cs, cr);
-  const int es = (tid >> 3) & 7;  // pass-1 epilogue role: row tid of D1
-  const int er = (((tid & 7) - es) & 7) + 8 * (tid >> 6);
   const unsigned lane_base = (unsigned)(32 * (warp & 3)) << 16;
-  unsigned mph = 0;
-  bool fail = false, mma_out = false;
+  // converting role (per half): sequence (s, r = 32 h + cl), values m = 16 cm .. 16 cm + 15
+  const int cs = tid & 7, cl = (tid >> 3) & 31, cm = tid >> 8;
+  // pass-1 epilogue role (per half): block 2 h + eb, lanes of quarter warp mod 4, columns
+  // 32 ec .. 32 ec + 31 (channels n = 16 ec .. 16 ec + 15)
+  const int eb = (warp >> 2) & 1, ec = warp >> 3;
+  const int erow = 128 * eb + 32 * (warp & 3) + lane;  // row within the half
+  const int es = (erow >> 3) & 7;
+  const int erl = (((erow & 7) - es) & 7) + 8 * (erow >> 6);  // r mod 32
+  unsigned pend = 0;  // MMA groups committed and not yet waited for (bit k: bar[2 + k])
+  bool fail = false;
   int it = 0;
+
+  auto convert = [&](int h) {  // half h of the W tile, in place, to its rows of X (hi, lo)
+    const float2* src = (const float2*)(sm + h * SH::HALF);
+    float2 v[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = src[((16 * cm + i) * 32 + cl) * TS + cs];
+    __syncthreads();
+    const int row = umma_xrow(cs, 32 * h + cl) - 256 * h;
+    unsigned char* xr = sm + h * SH::HALF + (unsigned)(row >> 3) * SH::X_SBO + (unsigned)(row & 7) * 16u;
+#pragma unroll
+    for (int c4 = 0; c4 < 4; ++c4) {  // K chunk 4 cm + c4: x_m for m = 4 (4 cm + c4) .. + 3
+      uint4 hv, lv;
+      umma_split2(v[4 * c4].x, v[4 * c4].y, hv.x, lv.x);
+      umma_split2(v[4 * c4 + 1].x, v[4 * c4 + 1].y, hv.y, lv.y);
+      umma_split2(v[4 * c4 + 2].x, v[4 * c4 + 2].y, hv.z, lv.z);
+      umma_split2(v[4 * c4 + 3].x, v[4 * c4 + 3].y, hv.w, lv.w);
+      const unsigned kc = (unsigned)(4 * cm + c4) * 128u;
+      *reinterpret_cast<uint4*>(xr + kc) = hv;
+      *reinterpret_cast<uint4*>(xr + SH::X_PART + kc) = lv;
+    }
+    umma::fence_smem_to_async();
+    umma::fence_before_sync();
+    __syncthreads();
+  };
+  auto pass1 = [&](int h) {  // thread 0: blocks 2h, 2h + 1 x 4 K steps x 3 products
+    umma::fence_after_sync();
+#pragma unroll 1
+    for (int bb = 0; bb < 2; ++bb) {
+      const unsigned d = tbase + 64u * (unsigned)(2 * h + bb);
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const unsigned xa = sb + h * SH::HALF + (unsigned)bb * 16u * SH::X_SBO + (unsigned)t * 256u;
+        const unsigned ea = sb + SH::OFF_E32 + (unsigned)t * 256u;
+        const uint64_t xh = umma::sdesc(xa, SH::X_LBO, SH::X_SBO);
+        const uint64_t xl = umma::sdesc(xa + SH::X_PART, SH::X_LBO, SH::X_SBO);
+        const uint64_t eh = umma::sdesc(ea, SH::E32_LBO, SH::E32_SBO);
+        const uint64_t el = umma::sdesc(ea + SH::E32_PART, SH::E32_LBO, SH::E32_SBO);
+        umma::mma_bf16(d, xh, eh, idesc1, t > 0);
+        umma::mma_bf16(d, xh, el, idesc1, true);
+        umma::mma_bf16(d, xl, eh, idesc1, true);
+      }
+    }
+    umma::commit(&bar[2 + h]);
+  };
+  auto epilogue1 = [&](int h) {  // D1 rows of half h times the twiddle, to its K rows of Y
+    float d[32];
+    umma::ld32_wait(tbase + lane_base + 64u * (unsigned)(2 * h + eb) + 32u * (unsigned)ec, d);
+    const float2* twr = tw + (32 * h + erl) * SH::S1 + 16 * ec;
+    unsigned char* yre = sm + h * SH::HALF + (unsigned)(erl >> 3) * SH::Y_LBO + (unsigned)(erl & 7) * 16u;
+    unsigned char* yim = yre + 4u * SH::Y_LBO;  // K row 32 + (r mod 32)
+#pragma unroll
+    for (int g = 0; g < 2; ++g) {  // channels n = 16 ec + 8 g .. + 7
+      unsigned rh[4], rl[4], ih[4], il[4];
+#pragma unroll
+      for (int p = 0; p < 4; ++p) {
+        const int n0 = 8 * g + 2 * p;
+        const float2 y0 = cmul(make_float2(d[2 * n0], d[2 * n0 + 1]), twr[n0]);
+        const float2 y1 = cmul(make_float2(d[2 * n0 + 2], d[2 * n0 + 3]), twr[n0 + 1]);
+        umma_split2(y0.x, y1.x, rh[p], rl[p]);
+        umma_split2(y0.y, y1.y, ih[p], il[p]);
+      }
+      const unsigned nofs = (unsigned)(4 * es + 2 * ec + g) * SH::Y_SBO;  // N group (32 s + n) / 8
+      *reinterpret_cast<uint4*>(yre + nofs) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
+      *reinterpret_cast<uint4*>(yre + SH::Y_PART + nofs) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
+      *reinterpret_cast<uint4*>(yim + nofs) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
+      *reinterpret_cast<uint4*>(yim + SH::Y_PART + nofs) = make_uint4(il[0], il[1], il[2], il[3]);
+    }
+    umma::fence_smem_to_async();
+    umma::fence_before_sync();
+    __syncthreads();
+  };
+  auto pass2 = [&](int h) {  // thread 0: K steps 4h .. 4h + 3 x 3 products into D2
+    umma::fence_after_sync();
+#pragma unroll
+    for (int t4 = 0; t4 < 4; ++t4) {
+      const int t = 4 * h + t4;
+      const unsigned ea = sb + SH::OFF_E64 + (unsigned)t * 256u;
+      const unsigned ya = sb + h * SH::HALF + (unsigned)(2 * t4) * SH::Y_LBO;
+      const uint64_t eh = umma::sdesc(ea, SH::E64_LBO, SH::E64_SBO);
+      const uint64_t el = umma::sdesc(ea + SH::E64_PART, SH::E64_LBO, SH::E64_SBO);
+      const uint64_t yh = umma::sdesc(ya, SH::Y_LBO, SH::Y_SBO);
+      const uint64_t yl = umma::sdesc(ya + SH::Y_PART, SH::Y_LBO, SH::Y_SBO);
+      umma::mma_bf16(tbase + SH::D2_COL, eh, yh, idesc2, t > 0);
+      umma::mma_bf16(tbase + SH::D2_COL, eh, yl, idesc2, true);
+      umma::mma_bf16(tbase + SH::D2_COL, el, yh, idesc2, true);
+    }
+    umma::commit(&bar[4 + h]);
+  };
+  // waits for MMA group k (bar[2 + k]) of this tile; false if the wait ran out
+  auto mma_wait = [&](int k) {
+    const bool ok = mbar_wait_bounded(&bar[2 + k], (unsigned)(it & 1));
+    if (__syncthreads_or(!ok)) return false;
+    pend &= ~(1u << k);
+    umma::fence_after_sync();
+    return true;
+  };
+
   for (long long tile = first; tile < ntiles; tile += stride, ++it) {
-    const bool ok = mbar_wait_bounded(&bar[0], (unsigned)(it & 1));
-    if (__syncthreads_or(!ok)) { fail = true; break; }
     const int q = (int)(tile / ntna), nat = (int)(tile - (long long)q * ntna);
     const int na0 = nat * TS;
-    {  // the W tile to registers, then in place to X (hi, lo)
-      float2 v[P2];
-#pragma unroll
-      for (int m = 0; m < P2; ++m) v[m] = region[(cr + P1 * m) * TS + cs];
-      __syncthreads();
-      unsigned char* xr = sm + (unsigned)(crow >> 3) * SH::X_SBO + (unsigned)(crow & 7) * 16u;
-#pragma unroll
-      for (int kc = 0; kc < 8; ++kc) {  // K chunk kc: x_m for m = 4 kc .. 4 kc + 3
-        uint4 h, l;
-        umma_split2(v[4 * kc].x, v[4 * kc].y, h.x, l.x);
-        umma_split2(v[4 * kc + 1].x, v[4 * kc + 1].y, h.y, l.y);
-        umma_split2(v[4 * kc + 2].x, v[4 * kc + 2].y, h.z, l.z);
-        umma_split2(v[4 * kc + 3].x, v[4 * kc + 3].y, h.w, l.w);
-        *reinterpret_cast<uint4*>(xr + kc * 128) = h;
-        *reinterpret_cast<uint4*>(xr + SH::X_PART + kc * 128) = l;
-      }
-    }
-    umma::fence_smem_to_async();
-    umma::fence_before_sync();
-    __syncthreads();
-    if (tid == 0) {  // pass 1: 4 row blocks x 4 K steps x 3 products
-      umma::fence_after_sync();
-#pragma unroll 1
-      for (int b = 0; b < 4; ++b) {
-#pragma unroll
-        for (int t = 0; t < 4; ++t) {
-          const unsigned xa = sb + (unsigned)b * 16u * SH::X_SBO + (unsigned)t * 256u;
-          const unsigned ea = sb + SH::OFF_E32 + (unsigned)t * 256u;
-          const uint64_t xh = umma::sdesc(xa, SH::X_LBO, SH::X_SBO);
-          const uint64_t xl = umma::sdesc(xa + SH::X_PART, SH::X_LBO, SH::X_SBO);
-          const uint64_t eh = umma::sdesc(ea, SH::E32_LBO, SH::E32_SBO);
-          const uint64_t el = umma::sdesc(ea + SH::E32_PART, SH::E32_LBO, SH::E32_SBO);
-          umma::mma_bf16(tbase + 64u * b, xh, eh, idesc1, t > 0);
-          umma::mma_bf16(tbase + 64u * b, xh, el, idesc1, true);
-          umma::mma_bf16(tbase + 64u * b, xl, eh, idesc1, true);
-        }
-      }
-      umma::commit(&bar[1]);
-    }
-    bool okm = mbar_wait_bounded(&bar[1], mph);
-    mph ^= 1u;
-    if (__syncthreads_or(!okm)) { fail = mma_out = true; break; }
-    umma::fence_after_sync();
-    {  // pass-1 epilogue: row tid of D1 times the twiddle, to Y (hi, lo)
-      float d[64];
-      umma::ld64_wait(tbase + lane_base + 64u * (unsigned)(tid >> 7), d);
-      const float2* twr = tw + er * SH::S1;
-      unsigned char* yre = sm + (unsigned)(er >> 3) * SH::Y_LBO + (unsigned)(er & 7) * 16u;
-      unsigned char* yim = yre + 8u * SH::Y_LBO;  // K row 64 + er
-#pragma unroll
-      for (int g = 0; g < 4; ++g) {  // channels n = 8 g .. 8 g + 7
-        unsigned rh[4], rl[4], ih[4], il[4];
-#pragma unroll
-        for (int p = 0; p < 4; ++p) {
-          const int n0 = 8 * g + 2 * p;
-          const float2 y0 = cmul(make_float2(d[2 * n0], d[2 * n0 + 1]), twr[n0]);
-          const float2 y1 = cmul(make_float2(d[2 * n0 + 2], d[2 * n0 + 3]), twr[n0 + 1]);
-          umma_split2(y0.x, y1.x, rh[p], rl[p]);
-          umma_split2(y0.y, y1.y, ih[p], il[p]);
-        }
-        const unsigned nofs = (unsigned)(4 * es + g) * SH::Y_SBO;  // N group (32 es + 8 g) / 8
-        *reinterpret_cast<uint4*>(yre + nofs) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
-        *reinterpret_cast<uint4*>(yre + SH::Y_PART + nofs) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
-        *reinterpret_cast<uint4*>(yim + nofs) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
-        *reinterpret_cast<uint4*>(yim + SH::Y_PART + nofs) = make_uint4(il[0], il[1], il[2], il[3]);
-      }
-    }
-    umma::fence_smem_to_async();
-    umma::fence_before_sync();
-    __syncthreads();
-    if (tid == 0) {  // pass 2: 8 K steps x 3 products into columns 0..255
-      umma::fence_after_sync();
-#pragma unroll
-      for (int t = 0; t < 8; ++t) {
-        const unsigned ea = sb + SH::OFF_E64 + (unsigned)t * 256u;
-        const unsigned ya = sb + (unsigned)(2 * t) * SH::Y_LBO;
-        const uint64_t eh = umma::sdesc(ea, SH::E64_LBO, SH::E64_SBO);
-        const uint64_t el = umma::sdesc(ea + SH::E64_PART, SH::E64_LBO, SH::E64_SBO);
-        const uint64_t yh = umma::sdesc(ya, SH::Y_LBO, SH::Y_SBO);
-        const uint64_t yl = umma::sdesc(ya + SH::Y_PART, SH::Y_LBO, SH::Y_SBO);
-        umma::mma_bf16(tbase, eh, yh, idesc2, t > 0);
-        umma::mma_bf16(tbase, eh, yl, idesc2, true);
-        umma::mma_bf16(tbase, el, yh, idesc2, true);
-      }
-      umma::commit(&bar[1]);
-    }
-    okm = mbar_wait_bounded(&bar[1], mph);
-    mph ^= 1u;
-    if (__syncthreads_or(!okm)) { fail = mma_out = true; break; }
-    umma::fence_after_sync();
-    if (tid == 0 && tile + stride < ntiles) {  // Y is read: refill the region
+    const bool more = tile + stride < ntiles;
+    bool ok = mbar_wait_bounded(&bar[0], (unsigned)(it & 1));
+    if (__syncthreads_or(!ok)) { fail = true; break; }
+    convert(0);
+    if (tid == 0) pass1(0);
+    pend |= 1u;
+    ok = mbar_wait_bounded(&bar[1], (unsigned)(it & 1));
+    if (__syncthreads_or(!ok)) { fail = true; break; }
+    convert(1);  // overlaps pass 1 of half 0
+    if (tid == 0) pass1(1);
+    pend |= 2u;
+    if (!mma_wait(0)) { fail = true; break; }
+    epilogue1(0);  // overlaps pass 1 of half 1
+    if (tid == 0) pass2(0);
+    pend |= 4u;
+    if (!mma_wait(1)) { fail = true; break; }
+    epilogue1(1);  // overlaps pass 2 of half 0
+    if (tid == 0) pass2(1);
+    pend |= 8u;
+    if (!mma_wait(2)) { fail = true; break; }
+    if (tid == 0 && more) {  // half 0 is read: refill it with the next tile's
       umma::fence_smem_to_async();
-      issue(tile + stride);
+      issue(tile + stride, 0);
+    }
+    if (!mma_wait(3)) { fail = true; break; }
+    if (tid == 0 && more) {
+      umma::fence_smem_to_async();
+      issue(tile + stride, 1);
     }
     {  // pass-2 epilogue: lane (re/im, c) of D2, channels n = 8 (warp / 4) .. + 7, 8 residues
       const int co = (warp & 3) >> 1, c = 32 * (warp & 1) + lane, ng = warp >> 2;
       const int j = 2 * q;
       float z[64];  // z[8 s + i]: channel 8 ng + i of residue s
-      umma::ld8x8_wait<32>(tbase + lane_base + 8u * (unsigned)ng, z);
+      umma::ld8x8_wait<32>(tbase + SH::D2_COL + lane_base + 8u * (unsigned)ng, z);
       if (co == 0 || j + 1 < Nr) {
         // The 8 residues of one (rate, channel) are one 32-byte sector.  Lanes 2k and 2k + 1
         // (channels c, c + 1) write both halves of one sector per instruction: the even
@@ -2391,9 +2440,10 @@ zdtf_output_umma_kernel(const __grid_constant__ CUtensorMap wmap, long long N, i
   }
   if (fail) {
     if (tid == 0) atomicOr(&g_fused_fault, 16);
-    // an MMA group whose wait ran out may still be running: give it one more bounded wait
-    // before its tensor memory is freed
-    if (mma_out) (void)mbar_wait_bounded(&bar[1], mph ^ 1u);
+    // MMA groups still outstanding get one more bounded wait each before their tensor
+    // memory is freed
+    for (int k = 0; k < 4; ++k)
+      if (pend & (1u << k)) (void)mbar_wait_bounded(&bar[2 + k], (unsigned)(it & 1));
   }
   umma::fence_before_sync();
   __syncthreads();
@@ -2837,6 +2887,22 @@ static bool w_tensor_map(CUtensorMap* map, const float2* W, int64_t Q, int64_t r
              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// Tensor map of W for P = 2048 as a 3-D float32 array (2 Q floats, r < 64, 32 * pair + m):
+// row k1 = r + 64 m of rate pair q is (r, 32 q + m).  Box {16 floats, 32 r, 32 m}: 8 residues
+// of one half (r < 32 or r >= 32) of a tile, 64 KB.
+static bool w_tensor_map_halves(CUtensorMap* map, const float2* W, int64_t Q, int64_t npairs) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc || ((uintptr_t)W & 15) != 0) return false;
+  const cuuint64_t dims[3] = {(cuuint64_t)(2 * Q), 64u, (cuuint64_t)(32 * npairs)};
+  const cuuint64_t strides[2] = {(cuuint64_t)(2 * Q * sizeof(float)),
+                                 (cuuint64_t)(64 * 2 * Q * sizeof(float))};
+  const cuuint32_t box[3] = {16u, 32u, 32u};
+  const cuuint32_t estr[3] = {1u, 1u, 1u};
+  return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void*)W, dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // FDR_NO_TMA=1 in the environment selects the register-load output kernel instead.
 static bool tma_output_enabled() {
   const char* e = getenv("FDR_NO_TMA");
@@ -2866,7 +2932,7 @@ int fused_output_mixed(const FusedPlan* st, const float2* W, float* dest, double
   if (st->P == 2048 && st->Q >= 8 && ((uintptr_t)dest & 15) == 0) {
     CUtensorMap map;
     using SH = OutUmmaShape;
-    if (w_tensor_map(&map, W, st->Q, st->npairs * (int64_t)st->P, SH::TS)) {
+    if (w_tensor_map_halves(&map, W, st->Q, st->npairs)) {
       const long long ntiles = (long long)(st->Q / SH::TS) * st->npairs;
       const int grid = (int)std::min<long long>(ntiles, sm_count());
       zdtf_output_umma_kernel<<<grid, SH::T, SH::SMEM, s>>>(
