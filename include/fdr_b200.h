@@ -58,12 +58,13 @@ typedef enum fdr_window {
 #define FDR_ZDT_EXACT_PHASE 0x2u    /* staged stages reduce chirp phases exactly (default:
                                        the reference's Float32 phase arguments) */
 #define FDR_ZDT_STAGED_ONLY 0x4u    /* fdr_zdt_execute always runs the staged kernels */
-#define FDR_ZDT_MIXED_PRECISION 0x8u /* fused path with P = 1024 (Nf = 2^19, and Nf = 2^20 with
-                                       Nt <= 16, which such a workspace splits as 1024 x 1024):
-                                       the inverse DFT_P runs as split-bfloat16 tensor-core
-                                       contractions with float32 accumulation (relative error
-                                       ~1e-5 of the FDR's peak instead of ~1e-6; no
-                                       counterpart in the reference) */
+#define FDR_ZDT_MIXED_PRECISION 0x8u /* fused path with P = 2048 (tcgen05, tensor-memory
+                                       accumulators; e.g. Nf = 2^20 and 2^21 with Nt <= 16) or
+                                       P = 1024 (mma.sync; e.g. Nf = 2^19): the inverse DFT_P
+                                       runs as split-bfloat16 tensor-core contractions with
+                                       float32 accumulation (relative error ~1e-5 of the FDR's
+                                       peak instead of ~1e-6; same split as without the flag;
+                                       no counterpart in the reference) */
 
 #define FDR_ZDT_FAST_STATS 0x10u     /* the snr statistics of the fused proto-hit scan
                                        (fdr_zdtfdr_protohits) come from float64 column moments
