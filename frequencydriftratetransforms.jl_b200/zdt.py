@@ -45,8 +45,9 @@ class ZDTWorkspace:
     of reproducing the reference's Float32 arguments in the staged stages),
     ``staged_only`` (zdtfdr_ always runs the staged kernels) and ``mixed_precision`` (the
     fused output pass runs its DFTs as split-bfloat16 tensor-core contractions where the
-    four-step split has P = 1024: Nf = 2^19 and, since such a workspace splits Nf = 2^20 as
-    1024 x 1024, Nf = 2^20 with Nt <= 16; ~1e-5 relative error instead of ~1e-6) and
+    four-step split has P = 2048, on tcgen05 with tensor-memory accumulators (e.g. Nf = 2^20
+    and 2^21 with Nt <= 16), or P = 1024, with mma.sync (e.g. Nf = 2^19); the split is the
+    same as without the flag; ~1e-5 relative error instead of ~1e-6) and
     ``fast_stats`` (the snr statistics of ``zdtfdr_protohits_`` come from float64 moments
     accumulated while the FDR is written: two fewer FDR reads, last bits of m and s may
     differ from the reference's Float32 values).
