@@ -378,11 +378,24 @@ int fdr_zdt_buffers(fdr_zdt* ws, void** F, void** Y, void** V) {
   return FDR_OK;
 }
 
+// The fused kernels read the spectrogram and write the FDR in 8-byte pairs of floats, so
+// their pointers must be 8-byte aligned (cudaMalloc'd and CuArray storage, and its columns
+// for even Nf, always are); any other pointer is rejected before a kernel is launched.
+static int check_pair_aligned(const void* p, const char* what) {
+  if ((reinterpret_cast<uintptr_t>(p) & 7) != 0) {
+    set_error(FDR_ERR_INVALID_ARGUMENT, "%s: the fused path needs an 8-byte aligned device "
+              "pointer (got %p)", what, p);
+    return FDR_ERR_INVALID_ARGUMENT;
+  }
+  return FDR_OK;
+}
+
 int fdr_zdt_input(fdr_zdt* ws, const float* spectrogram, fdr_stream_t stream) {
   FDR_CHECK_ARG(ws != nullptr, "input!: NULL workspace");
   FDR_CHECK_ARG(spectrogram != nullptr, "input!: spectrogram is NULL");
   cudaStream_t s = (cudaStream_t)stream;
   if (ws->fused) {
+    FDR_TRY(check_pair_aligned(spectrogram, "input!: spectrogram"));
     FDR_TRY(zdt_fused_input(ws, spectrogram, s));
     ws->A_valid = true;
     ws->F_valid = false;
@@ -425,13 +438,16 @@ static int zdt_execute(fdr_zdt* ws, const float* spectrogram, const float* r0s, 
   FDR_CHECK_ARG(window != FDR_WINDOW_CUSTOM || custom_window != nullptr,
                 "zdtfdr!: custom window values are NULL");
   for (int64_t b = 0; b < nbatch; ++b) FDR_CHECK_ARG(dests[b] != nullptr, "zdtfdr!: dests[%lld] is NULL", (long long)b);
+  const bool use_fused = ws->fused && !(ws->flags & FDR_ZDT_STAGED_ONLY);
+  if (use_fused)
+    for (int64_t b = 0; b < nbatch; ++b) FDR_TRY(check_pair_aligned(dests[b], "zdtfdr!: dest"));
+  if (ws->fused && spectrogram) FDR_TRY(check_pair_aligned(spectrogram, "zdtfdr!: spectrogram"));
   cudaStream_t s = (cudaStream_t)stream;
   zdt_mark(ws, "start", s);
   if (spectrogram) {
     FDR_TRY(fdr_zdt_input(ws, spectrogram, stream));
     zdt_mark(ws, "input", s);
   }
-  const bool use_fused = ws->fused && !(ws->flags & FDR_ZDT_STAGED_ONLY);
   for (int64_t b = 0; b < nbatch; ++b) {
     const float r0 = r0s ? r0s[b] : ws->r0;
     if (use_fused) {
@@ -464,6 +480,8 @@ static int zdt_execute_blocks(fdr_zdt* ws, const float* spectrogram, const int32
                   "zdtfdr blocks: block %lld = %d outside the workspace's %lld rates", (long long)i,
                   (int)blocks[i], (long long)ws->Nr);
   FDR_CHECK_ARG(4 * nblocks <= ws->W_pairs, "zdtfdr blocks: more than Nr/8 blocks");
+  FDR_TRY(check_pair_aligned(dest, "zdtfdr blocks: dest"));
+  if (spectrogram) FDR_TRY(check_pair_aligned(spectrogram, "zdtfdr blocks: spectrogram"));
   // the kernels take the rate index of each block's first rate
   std::vector<int> base((size_t)nblocks);
   for (int64_t i = 0; i < nblocks; ++i) base[(size_t)i] = 8 * (int)blocks[i];

@@ -131,6 +131,10 @@ int fdr_batch_create(fdr_batch** out, const fdr_batch_channel* channels, int64_t
     const auto& c = channels[i];
     FDR_CHECK_ARG(c.spectrogram && c.fdr && c.Nf >= 1 && c.Nt >= 1 && c.Nr >= 1,
                   "fdr_batch_create: channel %lld is invalid", (long long)i);
+    // the fused kernels move the spectrogram and the FDR in 8-byte pairs of floats
+    FDR_CHECK_ARG(((reinterpret_cast<uintptr_t>(c.spectrogram) | reinterpret_cast<uintptr_t>(c.fdr)) & 7) == 0,
+                  "fdr_batch_create: channel %lld: spectrogram and fdr must be 8-byte aligned",
+                  (long long)i);
   }
   fdr_batch* b = new fdr_batch();
   cudaGetDevice(&b->device);

@@ -16,7 +16,11 @@
  *  - Arrays are Julia column-major: an Nf x Nt spectrogram has channel (frequency) index
  *    fastest; element (n, t) of a matrix with leading dimension ld is at p[n + t*ld].
  *    Complex arrays are interleaved float pairs (ComplexF32).
- *  - Array arguments are DEVICE pointers unless the parameter says "host".
+ *  - Array arguments are DEVICE pointers unless the parameter says "host".  On the fused
+ *    ZDT path (zdtfdr!, its rate blocks, the fused proto-hit scan and the batch) the
+ *    spectrogram and the FDR destinations must be 8-byte aligned (cudaMalloc'd and CuArray
+ *    storage, and its columns for even Nf, are); other pointers are rejected with
+ *    FDR_ERR_INVALID_ARGUMENT before any kernel runs.
  *  - Work is ordered on the given CUDA stream (NULL = the legacy default stream) and is
  *    asynchronous unless the function says it synchronises (those that return values
  *    computed on the device to host variables).
